@@ -1,0 +1,413 @@
+"""Benchmark: reduce/scan GB/s and fraction of HBM peak at 2^28 elements.
+
+One step = the fp32 precision workload on 2^28 elements: transform_reduce
+dot product of two fp32 arrays (N(0,1), 1/8 of the values scaled by 1e-6)
+plus an inclusive scan of one fp32 |N(0,1)| array, inputs resident in HBM.
+Algorithmic bytes per step: dot 8n + scan 8n = 4 GiB.  Inputs (3 GiB) are
+larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (under torchrun): every rank runs its own replica of the step on its
+own GPU (weak scaling, no collective in the data path); the time is the max
+over ranks.  --impl reference times the reference algorithm's CPU
+implementation (the oracle port of the OpenMP backend's evaluation order)
+on the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N28 = 1 << 28
+N24 = 1 << 24
+GIB = float(1 << 30)
+METRIC = "reduce/scan GB/s & %HBM peak at 2^28; segmented batch calls/s, learned vs plain"
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of the dominant kernels from the committed ncu
+    summary (profiles/traffic.txt: `<kernel-key> <bytes-per-launch> <n>`)."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                out[parts[0]] = (float(parts[1]), int(parts[2]))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.count(",") >= 8]
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    import numpy as np
+
+    from opensycl_b200 import capi as C
+    from oracle import oracle as O
+
+    ns = 1 << 26  # bounded sample: 1/4 of the 2^28 workload per step
+    a = C.synth_fill(1, 1, ns, 0.125, 1e-6)
+    b = C.synth_fill(1, 2, ns, 0.125, 1e-6)
+    x = C.synth_fill(2, 3, ns, 0.125, 1e-6)
+    threads = O.num_threads()
+    step_bytes = 16.0 * ns
+
+    def step():
+        O.dot(O.F32, a, b, 0.0)
+        O.scan(O.F32, O.SUM, True, x)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    v = step_bytes * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "fp32 dot(2^28) + inclusive_scan(2^28), sample 2^26 per step",
+                   "sample_elems": ns},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"dot + inclusive_scan over 2^26 fp32 elements per step, "
+                                   f"OpenMP-backend evaluation order, {threads} threads"},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-ops", action="store_true", help="skip the per-primitive table")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+
+    from opensycl_b200 import capi as C
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    peak, peak_kind = hbm_peak()
+    n = N28
+    a_h = C.synth_fill(1, 1 + 10 * rank, n, 0.125, 1e-6)
+    b_h = C.synth_fill(1, 2 + 10 * rank, n, 0.125, 1e-6)
+    x_h = C.synth_fill(2, 3 + 10 * rank, n, 0.125, 1e-6)
+    a = torch.from_numpy(a_h).cuda()
+    b = torch.from_numpy(b_h).cuda()
+    x = torch.from_numpy(x_h).cuda()
+    y = torch.empty(n, dtype=torch.float32, device="cuda")
+    dres = torch.zeros(1, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    step_bytes = 8.0 * n + 8.0 * n
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        C.dot(a, b, init=0.0, out=dres)
+        if ev is not None:
+            ev[1].record(stream)
+        C.scan(x, True, "sum", None, out=y)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        end.record(stream)
+        barrier()
+    ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    dot_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    scan_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    clocks = clk.summary()
+
+    # parity of the timed results (one check, outside the timed region)
+    from_dot = dres.item()
+
+    value = step_bytes * args.steps * world / (ms / 1e3) / 1e9
+    kern = {"scan_kernel<f32,sum>": (scan_ms, 8.0 * n), "reduce_kernel<f32,dot>": (dot_ms, 8.0 * n)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_bytes = kern[dom]
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = read_traffic().get("scan_f32" if dom.startswith("scan") else "dot_f32")
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic[0] if traffic else None,
+                "algorithmic_bytes": dom_bytes}
+
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "fp32 dot(a,b) 2^28 + fp32 inclusive_scan 2^28 (config 2)",
+                   "elements": n, "step_bytes": step_bytes,
+                   "l2": "inputs (3 GiB) larger than the 126 MB L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roofline,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "per_kernel_ms": {"dot": round(dot_ms, 4), "scan": round(scan_ms, 4)},
+        "dot_result": from_dot,
+    }
+
+    if rank == 0 and world == 1:
+        result["e2e"] = measure_e2e(C, torch, a_h, b_h, x_h, args)
+        if not args.no_cpu:
+            result["cpu_baseline"] = cpu_baseline(a_h, b_h, x_h)
+        if not args.no_ops:
+            result["ops"] = measure_ops(C, torch, np, peak)
+    else:
+        result["e2e"] = None
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_e2e(C, torch, a_h, b_h, x_h, args):
+    """Same step through the C-ABI from pinned HOST buffers: copy the three
+    inputs in, run dot + scan, copy the dot result and the scan output back,
+    all inside the timed region."""
+    n = a_h.size
+    ap = torch.from_numpy(a_h).pin_memory()
+    bp = torch.from_numpy(b_h).pin_memory()
+    xp = torch.from_numpy(x_h).pin_memory()
+    yp = torch.empty(n, dtype=torch.float32).pin_memory()
+    rp = torch.empty(1, dtype=torch.float32).pin_memory()
+    a = torch.empty(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    x = torch.empty_like(a)
+    y = torch.empty_like(a)
+    r = torch.zeros(1, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream()
+
+    def step():
+        a.copy_(ap, non_blocking=True)
+        b.copy_(bp, non_blocking=True)
+        x.copy_(xp, non_blocking=True)
+        C.dot(a, b, init=0.0, out=r)
+        C.scan(x, True, "sum", None, out=y)
+        yp.copy_(y, non_blocking=True)
+        rp.copy_(r, non_blocking=True)
+
+    steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        step()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": round(16.0 * n / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n + 4,
+            "ms_per_step": round(ms, 3), "steps": steps,
+            "path": "pinned host -> cudaMemcpyAsync -> b2p_dot + b2p_scan -> host"}
+
+
+def cpu_baseline(a_h, b_h, x_h):
+    """Oracle port of the OpenMP-backend evaluation order on the host cores,
+    on a bounded sample (2^26 elements, ~10 s of CPU work at most)."""
+    from oracle import oracle as O
+
+    ns = 1 << 26
+    a, b, x = a_h[:ns], b_h[:ns], x_h[:ns]
+    threads = O.num_threads()
+    O.dot(O.F32, a, b, 0.0)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.dot(O.F32, a, b, 0.0)
+        O.scan(O.F32, O.SUM, True, x)
+        reps += 1
+        if time.perf_counter() - t0 > 8.0 or reps >= 20:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(16.0 * ns * reps / dt / 1e9, 3), "unit": "GB/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{reps} x (dot + inclusive_scan) over 2^26 fp32 elements, "
+                      f"OpenMP-backend evaluation order"}
+
+
+def _time_op(torch, fn, reps=10, warm=3, flush=None):
+    s = torch.cuda.current_stream()
+    for _ in range(warm):
+        fn()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def measure_ops(C, torch, np, peak):
+    """Per-primitive GB/s and fraction of measured HBM peak."""
+    ops = {}
+    n = N28
+
+    def rec(name, ms, nbytes, note=None):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        ops[name] = {"ms": round(ms, 4), "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
+                     "bytes": nbytes}
+        if note:
+            ops[name]["note"] = note
+
+    flush = torch.empty(1 << 27, dtype=torch.float32, device="cuda")  # 512 MB > L2
+    xi = torch.from_numpy(C.synth_fill(0, 0, n, -1000, 1000)).cuda()
+    yi = torch.empty_like(xi)
+    out = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rec("reduce_i32_2^28", _time_op(torch, lambda: C.reduce(xi, "sum", init=0, out=out)), 4 * n)
+    rec("scan_i32_2^28", _time_op(torch, lambda: C.scan(xi, True, "sum", None, out=yi)), 8 * n)
+    x24 = xi[:N24]
+    y24 = yi[:N24]
+    rec("reduce_i32_2^24_flushed", _time_op(torch, lambda: C.reduce(x24, "sum", init=0, out=out), flush=flush),
+        4 * N24, "L2 flushed before each rep")
+    rec("scan_i32_2^24_flushed", _time_op(torch, lambda: C.scan(x24, True, "sum", None, out=y24), flush=flush),
+        8 * N24, "L2 flushed before each rep")
+    del xi, yi
+    xf = torch.from_numpy(C.synth_fill(1, 1, n, 0.125, 1e-6)).cuda()
+    bf = torch.from_numpy(C.synth_fill(1, 2, n, 0.125, 1e-6)).cuda()
+    of = torch.zeros(1, dtype=torch.float32, device="cuda")
+    rec("reduce_f32_2^28", _time_op(torch, lambda: C.reduce(xf, "sum", init=0.0, out=of)), 4 * n)
+    rec("dot_f32_2^28", _time_op(torch, lambda: C.dot(xf, bf, out=of)), 8 * n)
+    yf = torch.empty_like(xf)
+    rec("scan_f32_2^28", _time_op(torch, lambda: C.scan(xf, True, "sum", None, out=yf)), 8 * n)
+    del bf
+    ab = torch.from_numpy(C.synth_fill(6, 1, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
+    bb = torch.from_numpy(C.synth_fill(6, 2, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
+    rec("dot_bf16_2^28", _time_op(torch, lambda: C.dot(ab, bb, out=of)), 4 * n)
+    rec("scan_bf16in_f32out_2^28", _time_op(torch, lambda: C.scan(ab, True, "sum", None, out=yf)), 6 * n)
+    del ab, bb, xf, yf
+    xu = torch.from_numpy(C.synth_fill(3, 4, n)).cuda()
+    yu = torch.empty_like(xu)
+    rec("exclusive_scan_u32_2^28", _time_op(torch, lambda: C.scan(xu, False, "sum", 0, out=yu)), 8 * n)
+    cnt = C.zeros(1, torch.uint64, "cuda")
+    C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt)
+    kept = int(cnt.item())
+    rec("copy_if_u32_2^28", _time_op(torch, lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt)),
+        4 * n + 4 * kept, f"kept {kept} ({kept / n:.4f})")
+    del xu, yu
+    k = torch.from_numpy(C.synth_fill(4, 5, n, 1.2)).cuda()
+    bins = torch.zeros(256, dtype=torch.int32, device="cuda")
+    rec("histogram_u8_zipf1.2_2^28", _time_op(torch, lambda: C.histogram_u8(k, bins=bins)), n + 1024)
+    ku = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda")
+    rec("histogram_u8_uniform_2^28", _time_op(torch, lambda: C.histogram_u8(ku, bins=bins)), n + 1024)
+    return ops
+
+
+if __name__ == "__main__":
+    main()

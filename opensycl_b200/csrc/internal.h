@@ -1,0 +1,85 @@
+// Host-side declarations shared by the translation units of libb2p.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/b2p.h"
+
+namespace b2p {
+
+struct LaunchConfig;
+
+// Cached per-device facts (queried once per device).
+struct DeviceInfo {
+  int device = -1;
+  int sm_count = 0;
+  int max_smem_optin = 0;
+  int cc_major = 0, cc_minor = 0;
+  char name[256] = {0};
+};
+const DeviceInfo &device_info();
+
+// Blocks per SM for (kernel, block, dynamic smem); cached.
+int occupancy(const void *kernel, int block, size_t smem);
+
+// Grid size for a launch that has `units` independent units of work
+// (tiles or runs) with `units_per_block` units per block.
+int grid_for(int grid_mode, long long units, int units_per_block, const void *kernel, int block,
+             size_t smem);
+
+// Raise a kernel's dynamic shared-memory limit once per (device, kernel).
+int ensure_dynamic_smem(const void *kernel, size_t bytes);
+
+// Wait bound for device-side spins (ns) and the stall test hook.
+uint64_t wait_timeout_ns();
+long long debug_stall_tile();
+
+// Record a CUDA failure; returns B2P_ERR_CUDA or B2P_OK.
+int cuda_status(cudaError_t e);
+
+// Reduce / dot.  b == nullptr: reduce; otherwise dot.
+size_t reduce_scratch_bytes(int dtype, size_t n, const void *a, const void *b);
+int launch_reduce(int dtype, int op, const void *a, const void *b, size_t n, void *out,
+                  const void *init, void *scratch, size_t scratch_bytes, int config,
+                  cudaStream_t s);
+
+// Scan and copy_if (decoupled look-back).
+size_t scan_scratch_bytes(int dtype, size_t n, int config);
+int launch_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
+                const void *init, void *scratch, size_t scratch_bytes, int config,
+                cudaStream_t s);
+size_t copy_if_scratch_bytes(int dtype, size_t n, int config);
+int launch_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
+                   uint64_t rhs, uint64_t *num_copied, void *scratch, size_t scratch_bytes,
+                   int config, cudaStream_t s);
+bool scan_config_valid(int dtype, int config);
+
+// Histogram.
+int launch_histogram_u8(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,
+                        cudaStream_t s);
+
+// Segmented reduce / scan (one persistent launch).
+size_t segmented_scratch_bytes(int dtype, size_t n, int64_t nseg, int config);
+int launch_segmented(int prim, int dtype, int op, int inclusive, const void *in, void *out,
+                     const int64_t *offsets, int64_t nseg, size_t total, const void *init,
+                     void *scratch, size_t scratch_bytes, int config, cudaStream_t s);
+bool segmented_config_valid(int dtype, int config);
+
+// Element sizes.
+inline size_t dtype_size(int dtype) {
+  switch (dtype) {
+  case B2P_I32: case B2P_U32: case B2P_F32: return 4;
+  case B2P_I64: case B2P_U64: case B2P_F64: return 8;
+  case B2P_BF16: return 2;
+  default: return 0;
+  }
+}
+// Size of the accumulation / output element (bf16 accumulates in fp32).
+inline size_t acc_size(int dtype) { return dtype == B2P_BF16 ? 4 : dtype_size(dtype); }
+inline bool dtype_is_float(int dtype) {
+  return dtype == B2P_F32 || dtype == B2P_BF16 || dtype == B2P_F64;
+}
+
+}  // namespace b2p

@@ -1,0 +1,116 @@
+"""C-ABI checks that need no GPU: the library loads, exports every function
+include/b2p.h declares, and its host-side logic (configuration table,
+scratch sizing, validation, synthetic inputs) behaves."""
+import ctypes
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from opensycl_b200 import capi as C
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+
+
+def test_library_exports_every_declared_function():
+    syms = subprocess.run(["nm", "-D", "--defined-only", C.LIB_PATH], capture_output=True,
+                          text=True, check=True).stdout
+    declared = C.header_functions()
+    assert len(declared) >= 30
+    missing = [f for f in declared if f" T {f}" not in syms]
+    assert not missing, missing
+    L = C.lib()
+    for f in declared:
+        assert hasattr(L, f)
+
+
+def test_library_is_sm100a_only():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", C.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+    assert "sm_90" not in out and "sm_80" not in out
+
+
+def test_config_table():
+    seen = set()
+    for c in range(C.NUM_CONFIGS):
+        b, it, g = C.config_describe(c)
+        assert b in (128, 256, 512, 1024) and it in (4, 8, 16, 32) and g in (0, 1, 2)
+        seen.add((b, it, g))
+    assert len(seen) == 48
+    with pytest.raises(C.B2PError):
+        C.config_describe(48)
+    L = C.lib()
+    # tiles above 8192 elements are masked for scans; reductions take all
+    assert sum(L.b2p_config_valid(C.PRIM_SCAN, C.F32, c) for c in range(48)) == 39
+    assert sum(L.b2p_config_valid(C.PRIM_REDUCE, C.F32, c) for c in range(48)) == 48
+    for prim in (C.PRIM_REDUCE, C.PRIM_SCAN, C.PRIM_COPY_IF, C.PRIM_HISTOGRAM):
+        c = L.b2p_heuristic_config(prim, C.F32, 1 << 20, 0)
+        assert L.b2p_config_valid(prim, C.F32, c)
+        a = L.b2p_auto_config(prim, C.F32, 1 << 20, 0, 0.0)
+        assert L.b2p_config_valid(prim, C.F32, a)
+
+
+def test_scratch_sizes():
+    L = C.lib()
+    # reduce: header + 8 bytes per run, runs bounded (~2368..4736) for large n
+    r28 = L.b2p_scratch_bytes(C.PRIM_REDUCE, C.F32, 1 << 28, 0, C.AUTO)
+    assert 256 < r28 < 256 + 8 * 2 * 4736 + 8 * 1024
+    assert L.b2p_scratch_bytes(C.PRIM_REDUCE, C.F32, 10, 0, C.AUTO) >= 264
+    # scan: header + 16 bytes per tile of the smallest tile (512 elements)
+    assert L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, 1 << 20, 0, C.AUTO) == 256 + 16 * 2048
+    b, it, _ = C.config_describe(5)
+    assert L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, 1 << 20, 0, 5) == 256 + 16 * ((1 << 20) // (b * it))
+
+
+def test_status_strings():
+    L = C.lib()
+    for s in range(9):
+        assert len(L.b2p_status_string(s)) > 0
+
+
+def test_synth_generator_pins():
+    pins = GOLD["synth"]
+    assert C.synth_fill(0, 0, 16, -1000, 1000).tolist() == pins["int32_seed0"]
+    got = C.synth_fill(1, 1, 16, 0.125, 1e-6)
+    assert np.array_equal(got, np.array(pins["fp32_seed1_frac0.125"], dtype=np.float32))
+    assert C.synth_fill(3, 4, 16).tolist() == pins["uint32_seed4"]
+
+
+def test_synth_distributions():
+    x = C.synth_fill(1, 1, 1 << 20, 0.125, 1e-6)
+    big = np.abs(x) > 1e-3
+    assert 0.86 < big.mean() < 0.89          # 1/8 replaced by 1e-6 * N(0,1)
+    assert abs(x[big].std() - 1.0) < 0.01
+    z = C.synth_fill(4, 5, 1 << 20, 1.2)
+    h = np.bincount(z, minlength=256) / z.size
+    H = sum(r ** -1.2 for r in range(1, 257))
+    assert abs(h[0] - 1 / H) < 0.005 and abs(h[1] - 2 ** -1.2 / H) < 0.005
+    b = C.synth_fill(6, 1, 1000, 0.125, 1e-6)
+    f = C.synth_fill(1, 1, 1000, 0.125, 1e-6)
+    back = (b.astype(np.uint32) << 16).view(np.float32)
+    assert np.all(np.abs(back - f) <= np.abs(f) * 2 ** -8)
+
+
+def test_synth_segments_cap():
+    offs = C.synth_segments(6, 10000, 20.0, 1 << 28)
+    lens = np.diff(offs)
+    assert offs[0] == 0 and offs[-1] <= 1 << 28 and offs[-1] > 0.99 * (1 << 28)
+    assert lens.min() >= 1 and lens.max() <= 1 << 20
+
+
+def test_calls_without_device_fail_cleanly():
+    """On a machine without a GPU every compute entry point returns an error
+    status instead of computing on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("host-only check")
+    L = C.lib()
+    buf = np.zeros(64, dtype=np.float32)
+    out = np.zeros(1, dtype=np.float32)
+    p = buf.ctypes.data_as(ctypes.c_void_p)
+    rc = L.b2p_reduce(C.F32, C.SUM, p, 64, out.ctypes.data_as(ctypes.c_void_p), None, p, 256, 0, None)
+    assert rc != C.OK
+    assert out[0] == 0

@@ -1,0 +1,48 @@
+"""Failure detection without a GPU fault: every look-back wait in the scan
+and copy_if kernels is bounded.  A test hook makes one tile never publish
+its status; its successors' waits run out after a short limit, the kernel
+records B2P_ERR_TIMEOUT in the scratch error word and returns, and the
+context stays usable for the next call.  No trap, no fault, no endless loop.
+"""
+import time
+
+import numpy as np
+import pytest
+import torch
+
+from opensycl_b200 import capi as C
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def short_timeout():
+    L = C.lib()
+    old = L.b2p_set_wait_timeout_ns(200_000_000)  # 0.2 s
+    yield
+    L.b2p_debug_stall_tile(-1)
+    L.b2p_set_wait_timeout_ns(old)
+
+
+@pytest.mark.parametrize("prim", ["scan", "copy_if"])
+def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim):
+    L = C.lib()
+    n = 512 * 200
+    x = torch.arange(n, dtype=torch.int32, device="cuda")
+    C.device_error(clear=True)
+    L.b2p_debug_stall_tile(37)
+    t0 = time.time()
+    if prim == "scan":
+        C.scan(x, True, "sum", None, config=0)  # 128 x 4 = 512-element tiles
+    else:
+        C.copy_if(x, 1, C.CMP_EQ, 0, config=0)
+    err = C.device_error(clear=True)
+    dt = time.time() - t0
+    L.b2p_debug_stall_tile(-1)
+    assert err == C.ERR_TIMEOUT
+    assert dt < 30.0
+    # the same scratch and context keep working
+    y = C.scan(x, True, "sum", None, config=0)
+    ref = np.cumsum(np.arange(n, dtype=np.int64)).astype(np.int32)
+    assert np.array_equal(y.cpu().numpy(), ref)
+    assert C.device_error(clear=True) == C.OK

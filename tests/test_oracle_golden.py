@@ -1,0 +1,138 @@
+"""Pins the CPU oracle (oracle/oracle.c) against the known answers of the
+reference's own tests (tests/golden/known_answers.json) and against plain
+numpy.  CPU only."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+
+
+@pytest.mark.parametrize("case", GOLD["pstl_reduce"], ids=lambda c: f"n{c['n']}")
+def test_pstl_reduce_known_answers(case):
+    n, dt = case["n"], (O.I32 if case["bits"] == 32 else O.I64)
+    x = np.arange(n, dtype=O.NP_OF[dt])
+    # the algorithms-library call leaves *out untouched for n == 0; the stdpar
+    # call returns init, which is what the golden value holds
+    got = O.reduce(dt, O.SUM, x, case["init"], out_init=case["init"]) if n else case["init"]
+    assert int(got) == case["expected"]
+    got2 = O.reduce(dt, O.SUM, x, 0, out_init=0) if n else 0
+    assert int(got2) == case["expected_noinit"]
+
+
+@pytest.mark.parametrize("case", [c for c in GOLD["pstl_scan"] if c["op"] == "plus"],
+                         ids=lambda c: f"n{c['n']}")
+def test_pstl_scan_plus_known_answers(case):
+    n = case["n"]
+    x = np.arange(n, dtype=np.int32)
+    if n == 0:
+        return
+    y = O.scan(O.I32, O.SUM, True, x)
+    assert int(y[-1]) == case["incl_last"]
+    assert int(y.astype(np.int64).view(np.uint64).sum(dtype=np.uint64)) == case["incl_sum_mod64"]
+    y = O.scan(O.I32, O.SUM, True, x, 3)
+    assert int(y[-1]) == case["incl_init_last"]
+    assert int(y.astype(np.int64).view(np.uint64).sum(dtype=np.uint64)) == case["incl_init_sum_mod64"]
+    y = O.scan(O.I32, O.SUM, False, x, 3)
+    assert int(y[-1]) == case["excl_last"]
+    assert int(y.astype(np.int64).view(np.uint64).sum(dtype=np.uint64)) == case["excl_sum_mod64"]
+
+
+@pytest.mark.parametrize("case", [c for c in GOLD["pstl_scan"] if c["op"] == "multiplies"],
+                         ids=lambda c: f"n{c['n']}")
+def test_pstl_scan_multiplies_known_answers(case):
+    n = case["n"]
+    if n == 0:
+        return
+    x = np.arange(n, dtype=np.int64)
+    y = O.scan(O.I64, O.PROD, True, x, 3)
+    assert not y.any()
+    y = O.scan(O.I64, O.PROD, False, x, 3)
+    assert y[0] == case["excl_first"] and not y[1:].any()
+
+
+@pytest.mark.parametrize("case", GOLD["pstl_copy_if"], ids=lambda c: c["case"])
+def test_pstl_copy_if_known_answers(case):
+    n, gen = case["n"], case["gen"]
+    i = np.arange(n, dtype=np.uint32)
+    x = {"i": i, "i+3": i + 3, "1": np.ones(n, np.uint32), "2i": 2 * i}[gen]
+    out, cnt = O.copy_if_u32(x, 1, 2, 0)  # (x & 1) == 0
+    assert cnt == case["count"]
+    assert int(out.astype(np.int64).sum()) == case["kept_sum"]
+    assert list(out[:3]) == case["kept_first"]
+
+
+@pytest.mark.parametrize("case", [c for c in GOLD["sycl_reduction"] if "plus" in c],
+                         ids=lambda c: f"{c['type']}-n{c['n']}")
+def test_sycl_reduction_known_answers(case):
+    n = case["n"]
+    i = np.arange(n)
+    plus = i
+    mul = np.where((i <= 1500) & (i % 100 == 0), 2, 1)
+    dt = {"int32": O.I32, "uint32": O.U32, "int64": O.I64, "float": O.F32}[case["type"]]
+    npd = O.NP_OF[dt]
+    s = O.reduce(dt, O.SUM, plus.astype(npd), 0)
+    p = O.reduce(dt, O.PROD, mul.astype(npd), 1)
+    if case["type"] == "float":
+        assert abs(float(s) - case["plus"]) <= case["rel_tol"] * abs(case["plus"])
+        assert abs(float(p) - case["multiplies"]) <= case["rel_tol"] * abs(case["multiplies"])
+    else:
+        assert int(s) == case["plus"]
+        assert int(p) == case["multiplies"]
+
+
+def test_sycl_reduction_iota_1024():
+    case = [c for c in GOLD["sycl_reduction"] if "iota_sum" in c][0]
+    x = np.arange(1024, dtype=np.int32)
+    assert int(O.reduce(O.I32, O.SUM, x, 0)) == case["iota_sum"]
+    assert int(O.reduce(O.I32, O.MAX, x, np.iinfo(np.int32).min)) == case["iota_max"]
+
+
+def test_atomic_fetch_add_known_answer():
+    case = GOLD["atomic"][0]
+    x = -np.arange(1, case["n"], dtype=np.int64)
+    assert int(O.reduce(O.I64, O.SUM, x, 0)) == case["fetch_add_expected"]
+
+
+def test_histogram_matches_bincount():
+    rng = np.random.default_rng(1)
+    k = rng.integers(0, 256, 100003).astype(np.uint8)
+    assert (O.histogram_u8(k) == np.bincount(k, minlength=256)).all()
+    base = np.arange(256, dtype=np.uint32)
+    assert (O.histogram_u8(k, bins=base) == base + np.bincount(k, minlength=256)).all()
+
+
+def test_reference_quirks_are_restated():
+    # maximum<float> identity is numeric_limits<float>::min() (numeric.hpp:53)
+    x = -np.ones(10, dtype=np.float32)
+    assert O.reduce(O.F32, O.MAX, x, -5.0) == np.finfo(np.float32).tiny
+    # bit ops have no known identity and take the init-flag path
+    x = np.array([0b1100, 0b1010, 0b0110], dtype=np.uint32)
+    assert O.reduce(O.U32, O.AND, x, 0xFFFFFFFF) == 0
+    assert O.reduce(O.U32, O.XOR, x, 0) == 0b0000
+
+
+def test_float_omp_order_vs_fp64():
+    rng = np.random.default_rng(2)
+    x = np.abs(rng.standard_normal(1 << 20)).astype(np.float32)
+    ref, _ = O.fp64_sum(O.F32, x)
+    got = O.reduce(O.F32, O.SUM, x, 0.0)
+    assert abs(float(got) - ref) / ref < 1e-4  # plain fp32 tree is within 1e-4
+    y = O.scan(O.F32, O.SUM, True, x)
+    y64 = O.fp64_scan(O.F32, True, x)
+    assert np.max(np.abs(y - y64) / y64) < 1e-3
+
+
+def test_segmented_matches_per_segment_calls():
+    rng = np.random.default_rng(3)
+    offs = np.concatenate([[0], np.cumsum(rng.integers(0, 50, 40))]).astype(np.int64)
+    x = rng.integers(-100, 100, offs[-1]).astype(np.int64)
+    r = O.segmented_reduce(O.I64, O.SUM, x, offs)
+    assert all(int(r[s]) == int(x[offs[s]:offs[s + 1]].sum()) for s in range(40))
+    y = O.segmented_scan(O.I64, O.SUM, True, x, offs)
+    for s in range(40):
+        assert (y[offs[s]:offs[s + 1]] == np.cumsum(x[offs[s]:offs[s + 1]])).all()
