@@ -66,7 +66,7 @@ int occupancy(const void *kernel, int block, size_t smem) {
 }
 
 int ensure_dynamic_smem(const void *kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return B2P_OK;
+  if (bytes == 0) return B2P_OK;  // static + dynamic may exceed the default even below 48 KB
   const int dev = device_info().device;
   auto key = std::make_pair(dev, kernel);
   {
@@ -146,7 +146,7 @@ bool config_valid(int prim, int dtype, int config) {
   case B2P_PRIM_SCAN:
     return scan_config_valid(dtype, config);
   case B2P_PRIM_COPY_IF:
-    return scan_config_valid(dtype == B2P_BF16 ? B2P_I32 : dtype, config);
+    return copy_if_config_valid(dtype, config);
   case B2P_PRIM_SEG_REDUCE:
   case B2P_PRIM_SEG_SCAN:
     return segmented_config_valid(dtype, config);
@@ -207,7 +207,7 @@ size_t b2p_scratch_bytes(int prim, int dtype, size_t n, int64_t nseg, int config
   case B2P_PRIM_COPY_IF:
     return copy_if_scratch_bytes(dtype, n, config);
   case B2P_PRIM_HISTOGRAM:
-    return kHeaderBytes;
+    return kScratchPrefix;
   case B2P_PRIM_SEG_REDUCE:
   case B2P_PRIM_SEG_SCAN:
     return segmented_scratch_bytes(dtype, n, nseg, config);

@@ -77,16 +77,25 @@ __device__ __forceinline__ void st_status(StatusWord *p, unsigned long long payl
       : "memory");
 }
 
-// Per-call control block at the start of every scratch buffer.
+// Per-call control block at the start of every scratch buffer.  Every
+// launch that uses the scratch advances `epoch` (its last block does), and
+// every word a launch writes into the scratch body is a StatusWord tagged
+// with its epoch, so no launch can mistake another launch's words (of any
+// primitive) for its own.
 struct __align__(64) ScratchHeader {
-  unsigned int epoch;                // incremented by the last block of every launch
-  unsigned int done_ctr;             // block arrivals, atomicInc-wrapped
-  unsigned int error;                // sticky b2p_status of a device-side failure
-  unsigned int pad0;
-  unsigned long long tile_ctr;       // dynamic tile ids (reset by the last block)
+  unsigned long long epoch;     // launches so far (56 bits used in tags)
+  unsigned long long tile_ctr;  // dynamic tile ids (reset by the last block)
+  unsigned int done_ctr;        // block arrivals, atomicInc-wrapped
+  unsigned int error;           // sticky b2p_status of a device-side failure
   unsigned int pad[10];
 };
 constexpr size_t kHeaderBytes = 256;
+// Fixed block of arrival counters right after the header (two-phase
+// kernels).  Launches that use them leave them zero; nothing else writes
+// there, so their position never overlaps another launch's data.
+constexpr size_t kCounterSlots = 1024;
+// Start of the per-launch body (epoch-tagged words) in every scratch buffer.
+constexpr size_t kScratchPrefix = kHeaderBytes + kCounterSlots * 4;
 
 // ------------------------------------------------------- double-float
 

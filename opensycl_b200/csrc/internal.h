@@ -55,6 +55,7 @@ int launch_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask
                    uint64_t rhs, uint64_t *num_copied, void *scratch, size_t scratch_bytes,
                    int config, cudaStream_t s);
 bool scan_config_valid(int dtype, int config);
+bool copy_if_config_valid(int dtype, int config);
 
 // Histogram.
 int launch_histogram_u8(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,

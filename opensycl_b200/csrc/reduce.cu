@@ -37,7 +37,7 @@ struct ReduceParams {
   unsigned long long init_bits;
   int has_init;
   ScratchHeader *hdr;
-  unsigned long long *partials;
+  StatusWord *partials;  // one epoch-tagged word per run
 };
 
 constexpr int kFinalWidth = 512;
@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
   const In *b = DOT ? reinterpret_cast<const In *>(p.b) + p.head : nullptr;
   const long long nvec = (long long)p.nvec;
   const int B = min(p.B, kMaxB);
+  const unsigned long long epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
 
   for (long long run = gw; run < p.runs; run += tw) {
     Acc acc = P::identity();
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
     }
     if constexpr (P::kCompensated) acc = df_norm(acc);
     acc = warp_allreduce<P>(acc);
-    if (lane == 0) p.partials[run] = P::pack(acc);
+    if (lane == 0) st_status(p.partials + run, P::pack(acc), (epoch << 8) | kFlagAgg);
   }
 
   // ---- last block to arrive combines everything (no waiting).
@@ -168,16 +169,16 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
     Acc acc = P::identity();
     long long r = v;
     for (; r + 3 * kFinalWidth < p.runs; r += 4 * kFinalWidth) {
-      unsigned long long x0 = __ldcg(p.partials + r);
-      unsigned long long x1 = __ldcg(p.partials + r + kFinalWidth);
-      unsigned long long x2 = __ldcg(p.partials + r + 2 * kFinalWidth);
-      unsigned long long x3 = __ldcg(p.partials + r + 3 * kFinalWidth);
+      unsigned long long x0 = ld_status(p.partials + r).payload;
+      unsigned long long x1 = ld_status(p.partials + r + kFinalWidth).payload;
+      unsigned long long x2 = ld_status(p.partials + r + 2 * kFinalWidth).payload;
+      unsigned long long x3 = ld_status(p.partials + r + 3 * kFinalWidth).payload;
       acc = P::combine(acc, P::unpack(x0));
       acc = P::combine(acc, P::unpack(x1));
       acc = P::combine(acc, P::unpack(x2));
       acc = P::combine(acc, P::unpack(x3));
     }
-    for (; r < p.runs; r += kFinalWidth) acc = P::combine(acc, P::unpack(__ldcg(p.partials + r)));
+    for (; r < p.runs; r += kFinalWidth) acc = P::combine(acc, P::unpack(ld_status(p.partials + r).payload));
     s_v[v] = P::pack(acc);
   }
   __syncthreads();
@@ -203,6 +204,8 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
     Out *out = reinterpret_cast<Out *>(p.out);
     Out basev = p.has_init ? from_bits64<Out>(p.init_bits) : *out;
     *out = P::finalize(P::combine(P::from_out(basev), total));
+    // every block read the epoch before arriving; the next launch sees this
+    atomicAdd(&p.hdr->epoch, 1ull);
   }
 }
 
@@ -245,7 +248,7 @@ int launch_t(const void *a, const void *b, size_t n, void *out, const void *init
              size_t scratch_bytes, int config, cudaStream_t st) {
   using In = typename P::In;
   Shape sh = reduce_shape(sizeof(In), n, a, DOT ? b : nullptr);
-  size_t need = kHeaderBytes + (size_t)std::max<long long>(sh.runs, 1) * 8;
+  size_t need = kScratchPrefix + (size_t)std::max<long long>(sh.runs, 1) * sizeof(StatusWord);
   if (scratch_bytes < need || (reinterpret_cast<uintptr_t>(scratch) & 255)) return B2P_ERR_SCRATCH;
   LaunchConfig lc = describe_config(config);
   ReduceParams p{};
@@ -265,7 +268,7 @@ int launch_t(const void *a, const void *b, size_t n, void *out, const void *init
   p.init_bits = 0;
   if (init) memcpy(&p.init_bits, init, sizeof(typename P::Out));
   p.hdr = reinterpret_cast<ScratchHeader *>(scratch);
-  p.partials = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(scratch) + kHeaderBytes);
+  p.partials = reinterpret_cast<StatusWord *>(reinterpret_cast<char *>(scratch) + kScratchPrefix);
   int wpb = lc.block / 32;
   if constexpr (DOT) {
     if (!sh.vec) {
@@ -321,7 +324,7 @@ size_t reduce_scratch_bytes(int dtype, size_t n, const void *a, const void *b) {
     Shape s2 = reduce_shape(es, n, (const void *)(uintptr_t)16, (const void *)(uintptr_t)8);
     sh.runs = std::max(sh.runs, s2.runs);
   }
-  return kHeaderBytes + (size_t)std::max<long long>(sh.runs, 1) * 8;
+  return kScratchPrefix + (size_t)std::max<long long>(sh.runs, 1) * sizeof(StatusWord);
 }
 
 int launch_reduce(int dtype, int op, const void *a, const void *b, size_t n, void *out,

@@ -1,4 +1,4 @@
-// Single-pass scan and order-preserving copy_if (decoupled look-back).
+// Scan and order-preserving copy_if.
 //
 // Replaces algorithms/scan/decoupled_lookback_scan.hpp:555-655 (init kernel
 // + main kernel of 128 work-items x 16 items, Kogge-Stone in local memory,
@@ -6,25 +6,34 @@
 // spin at :244-246) and the copy_if built on it (algorithms/algorithm.hpp:
 // 178-243, a 64-bit exclusive flag scan that reads the input twice).
 //
-// Here, per tile of BLOCK x ITEMS elements:
-//   1. dynamic tile id (atomicAdd), so a tile's predecessors have all
-//      started before it waits on them;
-//   2. 16-byte coalesced loads into a swizzled shared-memory tile, then each
-//      thread scans ITEMS consecutive elements in registers (fp32/bf16 SUM
-//      with compensated TwoSum arithmetic);
-//   3. block scan of the thread totals with warp shuffles;
-//   4. warp 0 publishes the tile aggregate and runs a warp-parallel
-//      look-back over 32 predecessors per step.  Status and payload share one
-//      128-bit word tagged with the launch's epoch, so stale words from an
-//      earlier launch are never mistaken for current ones and the status
-//      array never needs clearing.  Every wait is bounded (%globaltimer);
-//      on time-out the chain is marked broken and the error is recorded;
-//   5. outputs go back through the shared tile for coalesced stores.
-// fp32/bf16 SUM scans longer than 2^24 carry the cross-tile prefix in FP64.
-#include "common.cuh"
+// Two kernel families, chosen by the launch configuration's grid mode:
+//
+// * grid mode 0 -- decoupled look-back (the reference's algorithm, made
+//   bounded): per tile of BLOCK x ITEMS elements, a dynamic tile id,
+//   16-byte loads into a swizzled shared tile, a blocked per-thread scan, a
+//   block scan, then warp 0 publishes the tile aggregate and runs a
+//   warp-parallel look-back over 128 predecessors per step on epoch-tagged
+//   128-bit status words.  One launch, 2 x n element traffic; its speed is
+//   bounded by how fast prefixes propagate between tiles.
+//
+// * grid modes 1, 2 -- L2-blocked two-phase scan (persistent blocks): the
+//   input is cut into chunks of ~16 MB that stay resident in the 126 MB L2.
+//   Phase 1 of chunk k reduces each tile (DRAM read, L2 evict_last) and
+//   publishes its total; the last block to finish chunk k scans the chunk's
+//   tile totals into per-tile prefixes and marks the chunk ready.  Phase 2
+//   re-reads each tile from L2 (evict_first), scans it from its prefix and
+//   streams the output to DRAM.  One work queue orders phase 1 of chunk
+//   k + 2 before phase 2 of chunk k, so blocks never wait on a chain of
+//   predecessors and DRAM still moves only the algorithmic 2 x n elements.
+//
+// fp32/bf16 SUM accumulates with compensated (TwoSum) arithmetic; scans
+// longer than 2^24 carry cross-tile prefixes in FP64.  All waits are bounded
+// and report B2P_ERR_TIMEOUT through the scratch error word.
+#include "tile.cuh"
 #include "internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace b2p {
 
@@ -39,7 +48,11 @@ struct ScanParams {
   int vec_in;                    // input 16-byte aligned
   int vec_out;                   // output 16-byte aligned
   ScratchHeader *hdr;
-  StatusWord *status;
+  StatusWord *status;            // one word per tile
+  StatusWord *chunk_status;      // two-phase: one word per chunk
+  unsigned *counters;            // two-phase: phase-1 arrivals per chunk
+  long long chunk_tiles, nchunks;
+  int lookahead;
   unsigned long long timeout_ns;
   long long stall_tile;
   // copy_if
@@ -48,222 +61,210 @@ struct ScanParams {
   unsigned long long *num_copied;
 };
 
-// 16-byte-granular XOR swizzle of the shared tile: vector v lives in slot
-// v ^ ((v >> 3) & 7).  Conflict-free for striped 16-byte writes and for
-// blocked 16-byte reads of 1, 2, 4 or 8 vectors per thread.
-__device__ __forceinline__ int swz(int v) { return v ^ ((v >> 3) & 7); }
+// ------------------------------------------------------- per-tile phases
 
-template <class T>
-__device__ __forceinline__ T *smem_elem_ptr(char *tile, int i) {
-  const int byte = i * (int)sizeof(T);
-  return reinterpret_cast<T *>(tile + swz(byte >> 4) * 16 + (byte & 15));
-}
-
-// Load `count` elements of a tile into the swizzled shared buffer.
-template <class T>
-__device__ __forceinline__ void load_tile(char *tile, const T *src, int count, int tile_elems,
-                                          bool vec) {
-  if (vec && count == tile_elems) {
-    const int nv = tile_elems * (int)sizeof(T) / 16;
-    const uint4 *s = reinterpret_cast<const uint4 *>(src);
-    for (int v = threadIdx.x; v < nv; v += blockDim.x)
-      *reinterpret_cast<uint4 *>(tile + swz(v) * 16) = ld_stream_v4(s + v);
-  } else {
-    for (int i = threadIdx.x; i < count; i += blockDim.x) *smem_elem_ptr<T>(tile, i) = src[i];
+// Thread total of this thread's ITEMS consecutive elements of the shared
+// tile (blocked arrangement, 16-byte reads).
+template <class P, int ITEMS>
+__device__ __forceinline__ typename P::Acc thread_total(const char *buf, int count) {
+  using In = typename P::In;
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+  const int first = threadIdx.x * ITEMS;
+  typename P::Acc agg = P::identity();
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&w);
+#pragma unroll
+    for (int q = 0; q < IPV; ++q)
+      if (first + k * IPV + q < count) P::add(agg, e[q]);
   }
+  if constexpr (P::kCompensated) agg = df_norm(agg);
+  return agg;
 }
 
-// Store `count` elements from the swizzled shared buffer.
-template <class T>
-__device__ __forceinline__ void store_tile(const char *tile, T *dst, int count, int tile_elems,
-                                           bool vec) {
-  if (vec && count == tile_elems) {
-    const int nv = tile_elems * (int)sizeof(T) / 16;
-    uint4 *d = reinterpret_cast<uint4 *>(dst);
-    for (int v = threadIdx.x; v < nv; v += blockDim.x)
-      st_stream_v4(d + v, *reinterpret_cast<const uint4 *>(tile + swz(v) * 16));
-  } else {
-    for (int i = threadIdx.x; i < count; i += blockDim.x)
-      dst[i] = *smem_elem_ptr<T>(const_cast<char *>(tile), i);
-  }
-}
-
-// Read this thread's ITEMS consecutive elements (blocked arrangement).
-template <class T, int ITEMS>
-__device__ __forceinline__ void read_blocked(const char *tile, T (&x)[ITEMS]) {
-  constexpr int BYTES = ITEMS * (int)sizeof(T);
-  const int t = threadIdx.x;
-  if constexpr (BYTES % 16 == 0) {
-    constexpr int VPT = BYTES / 16;
+// Re-read the inputs and write the outputs one 16-byte vector at a time.
+// With equal element sizes each output vector overwrites the input vector
+// it came from, which only this thread reads.
+template <class P, int ITEMS>
+__device__ __forceinline__ void emit_scan(const char *buf, char *obuf, typename P::Acc run,
+                                          bool inclusive) {
+  using In = typename P::In;
+  using Out = typename P::Out;
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int OPV = 16 / (int)sizeof(Out);
+  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+  constexpr int OUT_PER_IN = IPV / OPV;
 #pragma unroll
-    for (int k = 0; k < VPT; ++k) {
-      uint4 w = *reinterpret_cast<const uint4 *>(tile + swz(t * VPT + k) * 16);
-      const T *e = reinterpret_cast<const T *>(&w);
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&w);
 #pragma unroll
-      for (int j = 0; j < 16 / (int)sizeof(T); ++j) x[k * (16 / sizeof(T)) + j] = e[j];
-    }
-  } else {
+    for (int m = 0; m < OUT_PER_IN; ++m) {
+      uint4 o;
+      Out *oe = reinterpret_cast<Out *>(&o);
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) x[j] = *smem_elem_ptr<T>(const_cast<char *>(tile), t * ITEMS + j);
-  }
-}
-
-template <class T, int ITEMS>
-__device__ __forceinline__ void write_blocked(char *tile, const T (&y)[ITEMS]) {
-  constexpr int BYTES = ITEMS * (int)sizeof(T);
-  const int t = threadIdx.x;
-  if constexpr (BYTES % 16 == 0) {
-    constexpr int VPT = BYTES / 16;
-#pragma unroll
-    for (int k = 0; k < VPT; ++k) {
-      uint4 w;
-      T *e = reinterpret_cast<T *>(&w);
-#pragma unroll
-      for (int j = 0; j < 16 / (int)sizeof(T); ++j) e[j] = y[k * (16 / sizeof(T)) + j];
-      *reinterpret_cast<uint4 *>(tile + swz(t * VPT + k) * 16) = w;
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) *smem_elem_ptr<T>(tile, t * ITEMS + j) = y[j];
-  }
-}
-
-// ------------------------------------------------------------ look-back
-
-// Warp-parallel look-back (called by all 32 lanes of one warp).  Lane l
-// watches predecessor win - l.  The warp polls jointly and waits only for
-// the lanes nearer than the closest predecessor whose inclusive prefix is
-// published, then combines those payloads.  Every wait is bounded by
-// timeout_ns (%globaltimer, checked every 64 polls); lanes still missing at
-// the deadline count as broken links.  Returns the exclusive prefix; sets
-// err when the chain is broken.
-template <class Pub, class Ops>
-__device__ Pub lookback(const StatusWord *status, long long tile, unsigned long long epoch_tag,
-                        unsigned long long timeout_ns, bool &err) {
-  const int lane = threadIdx.x & 31;
-  Pub acc = Ops::identity();
-  long long win = tile - 1;
-  err = false;
-  uint64_t t0 = 0;
-  while (true) {
-    const long long pred = win - lane;
-    bool have = pred < 0;  // never needed: tile 0 always publishes a prefix
-    unsigned long long payload = 0, flags = have ? kFlagPrefix : 0;
-    unsigned stop_mask = 0;
-    for (unsigned it = 0;; ++it) {
-      if (!have) {
-        StatusWord w = ld_status(status + pred);
-        if ((w.meta & ~0xffull) == epoch_tag && (w.meta & (kFlagAgg | kFlagPrefix))) {
-          have = true;
-          payload = w.payload;
-          flags = w.meta & 0xff;
+      for (int q = 0; q < OPV; ++q) {
+        const In xv = e[m * OPV + q];
+        if (inclusive) {
+          P::add(run, xv);
+          oe[q] = P::finalize(run);
+        } else {
+          oe[q] = P::finalize(run);
+          P::add(run, xv);
         }
       }
-      const unsigned have_mask = __ballot_sync(0xffffffffu, have);
-      stop_mask = __ballot_sync(0xffffffffu, have && (flags & (kFlagPrefix | kFlagError)));
-      const unsigned need = stop_mask ? ((2u << (__ffs(stop_mask) - 1)) - 1u) : 0xffffffffu;
-      if ((have_mask & need) == need) break;
-      if (it >= 8) __nanosleep(it < 64 ? 32 : 256);
-      if ((it & 63) == 63) {
-        uint64_t now = __shfl_sync(0xffffffffu, globaltimer_ns(), 0);
-        if (t0 == 0) {
-          t0 = now;
-        } else if (now - t0 > timeout_ns) {
-          if (!have) {
-            have = true;
-            flags = kFlagError;
-          }
-        }
-      }
+      *reinterpret_cast<uint4 *>(obuf + swz((threadIdx.x * VPT + k) * OUT_PER_IN + m) * 16) = o;
     }
-    const int stop = stop_mask ? __ffs(stop_mask) - 1 : 31;
-    Pub v = (pred >= 0 && lane <= stop && !(flags & kFlagError)) ? Ops::unpack(payload)
-                                                                   : Ops::identity();
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) v = Ops::combine(v, shfl_xor(v, m));
-    acc = Ops::combine(v, acc);
-    if (stop_mask) {
-      const unsigned long long sf = __shfl_sync(0xffffffffu, flags, stop);
-      err = (sf & kFlagError) != 0;
-      return acc;
-    }
-    win -= 32;
   }
 }
 
-template <class P>
-struct AccOps {
-  using Pub = typename P::Acc;
-  __device__ static Pub identity() { return P::identity(); }
-  __device__ static Pub combine(Pub a, Pub b) { return P::combine(a, b); }
-  __device__ static Pub unpack(unsigned long long v) { return P::unpack(v); }
-  __device__ static unsigned long long pack(Pub v) { return P::pack(v); }
-};
-
-struct F64Ops {
-  __device__ static double identity() { return 0.0; }
-  __device__ static double combine(double a, double b) { return a + b; }
-  __device__ static double unpack(unsigned long long v) { return __longlong_as_double((long long)v); }
-  __device__ static unsigned long long pack(double v) { return (unsigned long long)__double_as_longlong(v); }
-};
-
-struct CountOps {
-  __device__ static unsigned long long identity() { return 0; }
-  __device__ static unsigned long long combine(unsigned long long a, unsigned long long b) {
-    return a + b;
+// Running value of a thread: carry (+) the thread's exclusive prefix.
+template <class P, bool WIDE>
+__device__ __forceinline__ typename P::Acc start_value(unsigned long long carry_bits,
+                                                       typename P::Acc texcl) {
+  if constexpr (WIDE) {
+    const double c = F64Ops::unpack(carry_bits) + ((double)texcl.hi + (double)texcl.lo);
+    const float h = (float)c;
+    return DF{h, (float)(c - (double)h)};
+  } else {
+    return P::combine(P::unpack(carry_bits), texcl);
   }
-  __device__ static unsigned long long unpack(unsigned long long v) { return v; }
-  __device__ static unsigned long long pack(unsigned long long v) { return v; }
-};
-
-__device__ __forceinline__ void record_error(ScratchHeader *hdr, unsigned code) {
-  atomicCAS(&hdr->error, 0u, code);
 }
 
-// Persistent-loop prologue/epilogue shared by scan and copy_if.
-struct TileLoop {
-  unsigned long long epoch_tag;
-  unsigned epoch;
+template <class P, bool WIDE>
+__device__ __forceinline__ unsigned long long publish_value(typename P::Acc a) {
+  if constexpr (WIDE) return F64Ops::pack((double)a.hi + (double)a.lo);
+  else return P::pack(a);
+}
+
+template <class P, bool WIDE>
+__device__ __forceinline__ unsigned long long init_value(const ScanParams &p) {
+  using Out = typename P::Out;
+  if (!p.has_init) {
+    if constexpr (WIDE) return F64Ops::pack(0.0);
+    else return P::pack(P::identity());
+  }
+  const Out v = from_bits64<Out>(p.init_bits);
+  if constexpr (WIDE) return F64Ops::pack((double)v);
+  else return P::pack(P::from_out(v));
+}
+
+// Work queue of the two-phase kernels.  Segments, in order:
+//   P1(0) .. P1(D-1), then P1(k), P2(k-D) for k = D .. K-1, then
+//   P2(K-D) .. P2(K-1)
+// where P1(k) / P2(k) hold the tiles of chunk k (CT each, the last chunk
+// may be shorter) and D = min(lookahead, K).
+struct WorkItem {
+  int phase;
+  long long chunk, tile;
 };
 
-__device__ __forceinline__ void finish_launch(ScratchHeader *hdr, unsigned epoch) {
-  __syncthreads();
+__device__ __forceinline__ WorkItem decode_work(long long w, long long ntiles, long long CT,
+                                                long long K, int lookahead) {
+  const long long D = lookahead < K ? lookahead : K;
+  const long long slast = ntiles - (K - 1) * CT;
+  const long long p1 = (K - 1 < D) ? K - 1 : D + 2 * (K - 1 - D);  // segment of P1(K-1)
+  const long long p2 = 2 * K - 1;                                    // segment of P2(K-1)
+  auto start = [&](long long s) {
+    return s * CT - (long long)((p1 < s) + (p2 < s)) * (CT - slast);
+  };
+  auto size = [&](long long s) { return (s == p1 || s == p2) ? slast : CT; };
+  long long s = w / CT;
+  if (s > 2 * K - 1) s = 2 * K - 1;
+  for (int guard = 0; guard < 8; ++guard) {
+    const long long st = start(s);
+    if (w < st) --s;
+    else if (w >= st + size(s)) ++s;
+    else break;
+  }
+  const long long j = w - start(s);
+  WorkItem it;
+  if (s < D) {
+    it.phase = 1;
+    it.chunk = s;
+  } else if (s - D < 2 * (K - D)) {
+    const long long u = s - D;
+    if ((u & 1) == 0) {
+      it.phase = 1;
+      it.chunk = D + u / 2;
+    } else {
+      it.phase = 2;
+      it.chunk = u / 2;
+    }
+  } else {
+    it.phase = 2;
+    it.chunk = K - D + (s - D - 2 * (K - D));
+  }
+  it.tile = it.chunk * CT + j;
+  return it;
+}
+
+// Last block of a chunk's phase 1: turn the chunk's tile totals into
+// per-tile exclusive prefixes and publish the chunk's running total.
+template <class Ops>
+__device__ void finalize_chunk(const ScanParams &p, long long k, unsigned long long epoch_tag,
+                               unsigned long long init_bits, typename Ops::Pub *s_pub,
+                               unsigned long long *s_bits, int *s_err) {
+  using Pub = typename Ops::Pub;
+  const long long c0 = k * p.chunk_tiles;
+  const long long S = min(p.chunk_tiles, p.ntiles - c0);
   if (threadIdx.x == 0) {
+    bool err = false;
+    *s_bits = k == 0 ? init_bits
+                     : wait_flag(p.chunk_status + (k - 1), epoch_tag, kFlagPrefix, p.timeout_ns, &err);
+    *s_err = err;
+  }
+  __syncthreads();
+  __threadfence();
+  Pub carry = Ops::unpack(*s_bits);
+  const bool err = *s_err != 0;
+  for (long long b = 0; b < S; b += blockDim.x) {
+    const long long i = b + threadIdx.x;
+    Pub v = i < S ? Ops::unpack(ld_status(p.status + c0 + i).payload) : Ops::identity();
+    Pub tot;
+    Pub ex = block_exclusive_scan<Ops>(v, s_pub, &tot);
+    if (i < S) st_status(p.status + c0 + i, Ops::pack(Ops::combine(carry, ex)), epoch_tag | kFlagPrefix);
+    carry = Ops::combine(carry, tot);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
     __threadfence();
-    unsigned t = atomicInc(&hdr->done_ctr, gridDim.x - 1);
-    if (t == gridDim.x - 1) {
-      // Every block has fetched its terminating tile id and read the epoch.
-      atomicExch(&hdr->tile_ctr, 0ull);
-      atomicExch(&hdr->epoch, epoch + 1);
-    }
+    st_status(p.chunk_status + k, Ops::pack(carry), epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
   }
 }
 
-// --------------------------------------------------------------- scan
+// ---------------------------------------------------------- scan kernels
 
 template <class P, int ITEMS, bool WIDE>
 __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
-    scan_kernel(ScanParams p) {
+    scan_lookback_kernel(ScanParams p) {
   using In = typename P::In;
   using Acc = typename P::Acc;
   using Out = typename P::Out;
   using Ops = typename std::conditional<WIDE, F64Ops, AccOps<P>>::type;
-  using Pub = decltype(Ops::identity());
+  using Pub = typename Ops::Pub;
+  constexpr bool kSame = sizeof(In) == sizeof(Out);
 
   extern __shared__ __align__(16) char smem[];
   __shared__ Acc s_warp[32];
-  __shared__ unsigned long long s_tile, s_carry;
-  __shared__ unsigned s_epoch;
-  __shared__ int s_has_carry;
+  __shared__ unsigned long long s_tile, s_carry, s_epoch;
 
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5;
   const int tile_elems = blockDim.x * ITEMS;
-  if (threadIdx.x == 0) s_epoch = *reinterpret_cast<volatile unsigned *>(&p.hdr->epoch);
-  __syncthreads();
-  const unsigned epoch = s_epoch;
-  const unsigned long long epoch_tag = (unsigned long long)epoch << 8;
+  char *buf = smem;
+  char *obuf = kSame ? smem : smem + tile_elems * (int)sizeof(In);
   const In *in = reinterpret_cast<const In *>(p.in);
   Out *out = reinterpret_cast<Out *>(p.out);
+  const unsigned long long pol = l2_policy_stream();
+
+  if (threadIdx.x == 0) s_epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
+  __syncthreads();
+  const unsigned long long epoch = s_epoch;
+  const unsigned long long epoch_tag = epoch << 8;
+  const unsigned long long init_bits = init_value<P, WIDE>(p);
 
   while (true) {
     if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->tile_ctr, 1ull);
@@ -272,104 +273,154 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
     if (tile >= p.ntiles) break;
     const unsigned long long base = (unsigned long long)tile * tile_elems;
     const int count = (int)min((unsigned long long)tile_elems, p.n - base);
-
-    load_tile<In>(smem, in + base, count, tile_elems, p.vec_in);
+    load_tile_smem<In>(buf, in + base, count, tile_elems, p.vec_in, pol);
     __syncthreads();
 
-    In x[ITEMS];
-    read_blocked<In, ITEMS>(smem, x);
-    Acc r[ITEMS];
-    const int first = threadIdx.x * ITEMS;
-    Acc run = P::identity();
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-      if (first + j < count) P::add(run, x[j]);
-      r[j] = run;
-    }
-    Acc agg = run;
-    if constexpr (P::kCompensated) agg = df_norm(agg);
+    const Acc agg = thread_total<P, ITEMS>(buf, count);
+    Acc tile_agg;
+    const Acc texcl = block_exclusive_scan<AccOps<P>>(agg, s_warp, &tile_agg);
 
-    // block scan of thread totals
-    Acc incl = warp_inclusive_scan<P>(agg, lane);
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
     if (warp == 0) {
-      Acc w = lane < nwarps ? s_warp[lane] : P::identity();
-      w = warp_inclusive_scan<P>(w, lane);
-      s_warp[lane] = w;
-    }
-    __syncthreads();
-    Acc texcl = shfl_up(incl, 1);
-    if (lane == 0) texcl = P::identity();
-    if (warp > 0) texcl = P::combine(s_warp[warp - 1], texcl);
-    const Acc tile_agg = s_warp[nwarps - 1];
-
-    // cross-tile prefix (warp 0)
-    if (warp == 0) {
-      Pub agg_pub;
-      if constexpr (WIDE) agg_pub = (double)tile_agg.hi + (double)tile_agg.lo;
-      else agg_pub = tile_agg;
+      const unsigned long long agg_bits = publish_value<P, WIDE>(tile_agg);
       const bool publish = tile != p.stall_tile;
-      Pub carry = Ops::identity();
-      unsigned long long has_carry = 0;
+      Pub carry;
       if (tile == 0) {
-        if (p.has_init) {
-          if constexpr (WIDE) carry = (double)from_bits64<Out>(p.init_bits);
-          else carry = P::from_out(from_bits64<Out>(p.init_bits));
-          has_carry = 1;
-        }
-        if (lane == 0 && publish)
-          st_status(p.status, Ops::pack(has_carry ? Ops::combine(carry, agg_pub) : agg_pub),
-                    epoch_tag | kFlagPrefix);
+        carry = Ops::unpack(init_bits);
+        if ((threadIdx.x & 31) == 0 && publish)
+          st_status(p.status, Ops::pack(Ops::combine(carry, Ops::unpack(agg_bits))), epoch_tag | kFlagPrefix);
       } else {
-        if (lane == 0 && publish)
-          st_status(p.status + tile, Ops::pack(agg_pub), epoch_tag | kFlagAgg);
+        if ((threadIdx.x & 31) == 0 && publish) st_status(p.status + tile, agg_bits, epoch_tag | kFlagAgg);
         bool err;
-        carry = lookback<Pub, Ops>(p.status, tile, epoch_tag, p.timeout_ns, err);
-        has_carry = 1;
-        if (lane == 0) {
+        carry = lookback<Ops>(p.status, tile, epoch_tag, p.timeout_ns, err);
+        if ((threadIdx.x & 31) == 0) {
           if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
           if (publish)
-            st_status(p.status + tile, Ops::pack(Ops::combine(carry, agg_pub)),
+            st_status(p.status + tile, Ops::pack(Ops::combine(carry, Ops::unpack(agg_bits))),
                       epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
         }
       }
-      if (lane == 0) {
-        s_carry = Ops::pack(carry);
-        s_has_carry = (int)has_carry;
-      }
+      if ((threadIdx.x & 31) == 0) s_carry = Ops::pack(carry);
     }
     __syncthreads();
-    const bool has_carry = s_has_carry != 0;
-    // base = carry (+) thread exclusive prefix
-    Acc basev = texcl;
-    if (has_carry) {
-      if constexpr (WIDE) {
-        double c = F64Ops::unpack(s_carry) + ((double)texcl.hi + (double)texcl.lo);
-        float h = (float)c;
-        basev = DF{h, (float)(c - (double)h)};
-      } else {
-        basev = P::combine(Ops::unpack(s_carry), texcl);
-      }
-    }
-    Out y[ITEMS];
-    if (p.inclusive) {
-#pragma unroll
-      for (int j = 0; j < ITEMS; ++j) y[j] = P::finalize(P::combine(basev, r[j]));
-    } else {
-      y[0] = P::finalize(basev);
-#pragma unroll
-      for (int j = 1; j < ITEMS; ++j) y[j] = P::finalize(P::combine(basev, r[j - 1]));
-    }
-    write_blocked<Out, ITEMS>(smem, y);
+    emit_scan<P, ITEMS>(buf, obuf, start_value<P, WIDE>(s_carry, texcl), p.inclusive);
     __syncthreads();
-    store_tile<Out>(smem, out + base, count, tile_elems, p.vec_out);
+    store_tile<Out>(obuf, out + base, count, tile_elems, p.vec_out);
     __syncthreads();
   }
-  finish_launch(p.hdr, epoch);
+  finish_launch(p.hdr, epoch, nullptr, 0);
 }
 
-// ------------------------------------------------------------ copy_if
+template <class P, int ITEMS, bool WIDE>
+__global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
+    scan_twophase_kernel(ScanParams p) {
+  using In = typename P::In;
+  using Acc = typename P::Acc;
+  using Out = typename P::Out;
+  using Ops = typename std::conditional<WIDE, F64Ops, AccOps<P>>::type;
+  using Pub = typename Ops::Pub;
+  constexpr bool kSame = sizeof(In) == sizeof(Out);
+
+  extern __shared__ __align__(16) char smem[];
+  __shared__ Acc s_warp[32];
+  __shared__ Pub s_pub[32];
+  __shared__ unsigned long long s_w[2], s_carry, s_epoch, s_bits;
+  __shared__ int s_fin, s_err;
+
+  const int tile_elems = blockDim.x * ITEMS;
+  const int in_bytes = tile_elems * (int)sizeof(In);
+  char *bufs[2] = {smem, smem + in_bytes};
+  char *obuf_sep = smem + 2 * in_bytes;
+  const In *in = reinterpret_cast<const In *>(p.in);
+  Out *out = reinterpret_cast<Out *>(p.out);
+  const unsigned long long keep = l2_policy_keep(), stream = l2_policy_stream();
+  const long long nitems = 2 * p.ntiles;
+
+  if (threadIdx.x == 0) {
+    s_epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
+    s_w[0] = atomicAdd(&p.hdr->tile_ctr, 1ull);
+  }
+  __syncthreads();
+  const unsigned long long epoch = s_epoch;
+  const unsigned long long epoch_tag = epoch << 8;
+  const unsigned long long init_bits = init_value<P, WIDE>(p);
+  long long known_ready = -1;  // chunks become ready in order
+
+  // Bring the input tile of work id w into buf (phase-1 reads are kept in
+  // L2 for phase 2; phase-2 reads release their lines).
+  auto prefetch = [&](long long w, char *buf) {
+    if (w < nitems) {
+      const WorkItem it = decode_work(w, p.ntiles, p.chunk_tiles, p.nchunks, p.lookahead);
+      if (it.tile >= 0 && it.tile < p.ntiles) {
+        const unsigned long long b = (unsigned long long)it.tile * tile_elems;
+        prefetch_tile<In>(buf, in + b, (int)min((unsigned long long)tile_elems, p.n - b), tile_elems,
+                          p.vec_in, it.phase == 1 ? keep : stream);
+        return;
+      }
+    }
+    cp_async_commit();
+  };
+  prefetch((long long)s_w[0], bufs[0]);
+
+  for (int i = 0;; ++i) {
+    const long long w = (long long)s_w[i & 1];
+    if (w >= nitems) break;
+    char *buf = bufs[i & 1];
+    if (threadIdx.x == 0) s_w[(i + 1) & 1] = atomicAdd(&p.hdr->tile_ctr, 1ull);
+    __syncthreads();
+    prefetch((long long)s_w[(i + 1) & 1], bufs[(i + 1) & 1]);
+    const WorkItem item = decode_work(w, p.ntiles, p.chunk_tiles, p.nchunks, p.lookahead);
+    const long long tile = item.tile;
+    if (tile < 0 || tile >= p.ntiles) {  // never taken: decode_work covers [0, 2 ntiles)
+      if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_INVALID_ARG);
+      cp_async_wait_1();
+      __syncthreads();
+      continue;
+    }
+    const unsigned long long base = (unsigned long long)tile * tile_elems;
+    const int count = (int)min((unsigned long long)tile_elems, p.n - base);
+    if (item.phase == 2 && threadIdx.x == 0) {
+      bool err = false;
+      if (item.chunk > known_ready) {
+        wait_flag(p.chunk_status + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
+        if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
+      }
+      s_carry = ld_status(p.status + tile).payload;
+    }
+    if (item.phase == 2) known_ready = max(known_ready, item.chunk);
+    cp_async_wait_1();  // this item's tile has landed
+    __syncthreads();
+
+    const Acc agg = thread_total<P, ITEMS>(buf, count);
+    Acc tile_agg;
+    const Acc texcl = block_exclusive_scan<AccOps<P>>(agg, s_warp, &tile_agg);
+    if (item.phase == 1) {
+      if (threadIdx.x == 0) {
+        int fin = 0;
+        if (tile != p.stall_tile) {
+          st_status(p.status + tile, publish_value<P, WIDE>(tile_agg), epoch_tag | kFlagAgg);
+          __threadfence();
+          const long long S = min(p.chunk_tiles, p.ntiles - item.chunk * p.chunk_tiles);
+          fin = atomicAdd(p.counters + item.chunk, 1u) == (unsigned)(S - 1);
+        }
+        s_fin = fin;
+      }
+      __syncthreads();
+      if (s_fin) {
+        __threadfence();
+        finalize_chunk<Ops>(p, item.chunk, epoch_tag, init_bits, s_pub, &s_bits, &s_err);
+      }
+    } else {
+      char *obuf = kSame ? buf : obuf_sep;
+      emit_scan<P, ITEMS>(buf, obuf, start_value<P, WIDE>(s_carry, texcl), p.inclusive);
+      __syncthreads();
+      store_tile<Out>(obuf, out + base, count, tile_elems, p.vec_out);
+    }
+    __syncthreads();
+  }
+  finish_launch(p.hdr, epoch, p.counters, p.nchunks);
+}
+
+// ------------------------------------------------------- copy_if kernels
 
 template <class T>
 __device__ __forceinline__ bool pred_bits(T v, unsigned long long mask, int cmp,
@@ -388,22 +439,67 @@ __device__ __forceinline__ bool pred_bits(T v, unsigned long long mask, int cmp,
   }
 }
 
+// Predicate flags of this thread's ITEMS consecutive elements.
+template <class T, int ITEMS>
+__device__ __forceinline__ unsigned thread_flags(const char *buf, int count, const ScanParams &p,
+                                                 int *kept) {
+  constexpr int EPV = 16 / (int)sizeof(T);
+  constexpr int VPT = ITEMS / EPV;
+  const int first = threadIdx.x * ITEMS;
+  unsigned keep = 0;
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const T *e = reinterpret_cast<const T *>(&w);
+#pragma unroll
+    for (int q = 0; q < EPV; ++q) {
+      const int j = k * EPV + q;
+      const bool kb = (first + j < count) && pred_bits(e[q], p.mask, p.cmp, p.rhs);
+      keep |= (unsigned)kb << j;
+      n += kb;
+    }
+  }
+  *kept = n;
+  return keep;
+}
+
+// Compact the kept elements of this thread into the staging tile at `o`.
+template <class T, int ITEMS>
+__device__ __forceinline__ void emit_kept(const char *buf, char *obuf, unsigned keep, int o) {
+  constexpr int EPV = 16 / (int)sizeof(T);
+  constexpr int VPT = ITEMS / EPV;
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    if ((keep >> (k * EPV)) & ((1u << EPV) - 1u)) {
+      const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+      const T *e = reinterpret_cast<const T *>(&w);
+#pragma unroll
+      for (int q = 0; q < EPV; ++q)
+        if (keep & (1u << (k * EPV + q))) *smem_elem_ptr<T>(obuf, o++) = e[q];
+    }
+  }
+}
+
 template <class T, int ITEMS>
 __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
-    copy_if_kernel(ScanParams p) {
+    copy_if_lookback_kernel(ScanParams p) {
   extern __shared__ __align__(16) char smem[];
-  __shared__ unsigned s_warp[32];
-  __shared__ unsigned long long s_tile, s_carry;
-  __shared__ unsigned s_epoch;
+  __shared__ unsigned long long s_warp[32];
+  __shared__ unsigned long long s_tile, s_carry, s_epoch;
 
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5;
   const int tile_elems = blockDim.x * ITEMS;
-  if (threadIdx.x == 0) s_epoch = *reinterpret_cast<volatile unsigned *>(&p.hdr->epoch);
-  __syncthreads();
-  const unsigned epoch = s_epoch;
-  const unsigned long long epoch_tag = (unsigned long long)epoch << 8;
+  char *buf = smem;
+  char *obuf = smem + tile_elems * (int)sizeof(T);
   const T *in = reinterpret_cast<const T *>(p.in);
   T *out = reinterpret_cast<T *>(p.out);
+  const unsigned long long pol = l2_policy_stream();
+
+  if (threadIdx.x == 0) s_epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
+  __syncthreads();
+  const unsigned long long epoch = s_epoch;
+  const unsigned long long epoch_tag = epoch << 8;
 
   while (true) {
     if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->tile_ctr, 1ull);
@@ -412,77 +508,147 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
     if (tile >= p.ntiles) break;
     const unsigned long long base = (unsigned long long)tile * tile_elems;
     const int count = (int)min((unsigned long long)tile_elems, p.n - base);
-
-    load_tile<T>(smem, in + base, count, tile_elems, p.vec_in);
+    load_tile_smem<T>(buf, in + base, count, tile_elems, p.vec_in, pol);
     __syncthreads();
-    T x[ITEMS];
-    read_blocked<T, ITEMS>(smem, x);
-    const int first = threadIdx.x * ITEMS;
-    unsigned keep = 0;
-    int kept = 0;
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-      bool k = (first + j < count) && pred_bits(x[j], p.mask, p.cmp, p.rhs);
-      keep |= (unsigned)k << j;
-      kept += k;
-    }
-    // block exclusive scan of per-thread counts
-    unsigned incl = (unsigned)kept;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      unsigned o = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= d) incl += o;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      unsigned w = lane < nwarps ? s_warp[lane] : 0;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        unsigned o = __shfl_up_sync(0xffffffffu, w, d);
-        if (lane >= d) w += o;
-      }
-      s_warp[lane] = w;
-    }
-    __syncthreads();
-    unsigned texcl = incl - (unsigned)kept + (warp > 0 ? s_warp[warp - 1] : 0u);
-    const unsigned tile_kept = s_warp[nwarps - 1];
+    int kept;
+    const unsigned keep = thread_flags<T, ITEMS>(buf, count, p, &kept);
+    unsigned long long tile_kept;
+    const unsigned long long texcl =
+        block_exclusive_scan<CountOps>((unsigned long long)kept, s_warp, &tile_kept);
 
     if (warp == 0) {
       const bool publish = tile != p.stall_tile;
       unsigned long long carry = 0;
       if (tile == 0) {
-        if (lane == 0 && publish) st_status(p.status, tile_kept, epoch_tag | kFlagPrefix);
+        if ((threadIdx.x & 31) == 0 && publish) st_status(p.status, tile_kept, epoch_tag | kFlagPrefix);
       } else {
-        if (lane == 0 && publish) st_status(p.status + tile, tile_kept, epoch_tag | kFlagAgg);
+        if ((threadIdx.x & 31) == 0 && publish) st_status(p.status + tile, tile_kept, epoch_tag | kFlagAgg);
         bool err;
-        carry = lookback<unsigned long long, CountOps>(p.status, tile, epoch_tag, p.timeout_ns, err);
-        if (lane == 0) {
+        carry = lookback<CountOps>(p.status, tile, epoch_tag, p.timeout_ns, err);
+        if ((threadIdx.x & 31) == 0) {
           if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
           if (publish)
             st_status(p.status + tile, carry + tile_kept,
                       epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
         }
       }
-      if (lane == 0) {
+      if ((threadIdx.x & 31) == 0) {
         s_carry = carry;
         if (tile == p.ntiles - 1 && p.num_copied) *p.num_copied = carry + tile_kept;
       }
     }
-    __syncthreads();  // everyone has read the input tile; reuse it for output
-    {
-      int o = (int)texcl;
-#pragma unroll
-      for (int j = 0; j < ITEMS; ++j)
-        if (keep & (1u << j)) *smem_elem_ptr<T>(smem, o++) = x[j];
-    }
+    emit_kept<T, ITEMS>(buf, obuf, keep, (int)texcl);
     __syncthreads();
     const unsigned long long obase = s_carry;
     for (int i = threadIdx.x; i < (int)tile_kept; i += blockDim.x)
-      out[obase + i] = *smem_elem_ptr<T>(smem, i);
+      out[obase + i] = *smem_elem_ptr<T>(obuf, i);
     __syncthreads();
   }
-  finish_launch(p.hdr, epoch);
+  finish_launch(p.hdr, epoch, nullptr, 0);
+}
+
+template <class T, int ITEMS>
+__global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
+    copy_if_twophase_kernel(ScanParams p) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ unsigned long long s_warp[32];
+  __shared__ unsigned long long s_w[2], s_carry, s_epoch, s_bits;
+  __shared__ int s_fin, s_err;
+
+  const int tile_elems = blockDim.x * ITEMS;
+  const int buf_bytes = tile_elems * (int)sizeof(T);
+  char *bufs[2] = {smem, smem + buf_bytes};
+  char *obuf = smem + 2 * buf_bytes;  // compacted output staging
+  const T *in = reinterpret_cast<const T *>(p.in);
+  T *out = reinterpret_cast<T *>(p.out);
+  const unsigned long long keepp = l2_policy_keep(), stream = l2_policy_stream();
+  const long long nitems = 2 * p.ntiles;
+
+  if (threadIdx.x == 0) {
+    s_epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
+    s_w[0] = atomicAdd(&p.hdr->tile_ctr, 1ull);
+  }
+  __syncthreads();
+  const unsigned long long epoch = s_epoch;
+  const unsigned long long epoch_tag = epoch << 8;
+  long long known_ready = -1;
+
+  auto prefetch = [&](long long w, char *buf) {
+    if (w < nitems) {
+      const WorkItem it = decode_work(w, p.ntiles, p.chunk_tiles, p.nchunks, p.lookahead);
+      if (it.tile >= 0 && it.tile < p.ntiles) {
+        const unsigned long long b = (unsigned long long)it.tile * tile_elems;
+        prefetch_tile<T>(buf, in + b, (int)min((unsigned long long)tile_elems, p.n - b), tile_elems,
+                         p.vec_in, it.phase == 1 ? keepp : stream);
+        return;
+      }
+    }
+    cp_async_commit();
+  };
+  prefetch((long long)s_w[0], bufs[0]);
+
+  for (int i = 0;; ++i) {
+    const long long w = (long long)s_w[i & 1];
+    if (w >= nitems) break;
+    char *buf = bufs[i & 1];
+    if (threadIdx.x == 0) s_w[(i + 1) & 1] = atomicAdd(&p.hdr->tile_ctr, 1ull);
+    __syncthreads();
+    prefetch((long long)s_w[(i + 1) & 1], bufs[(i + 1) & 1]);
+    const WorkItem item = decode_work(w, p.ntiles, p.chunk_tiles, p.nchunks, p.lookahead);
+    const long long tile = item.tile;
+    if (tile < 0 || tile >= p.ntiles) {  // never taken: decode_work covers [0, 2 ntiles)
+      if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_INVALID_ARG);
+      cp_async_wait_1();
+      __syncthreads();
+      continue;
+    }
+    const unsigned long long base = (unsigned long long)tile * tile_elems;
+    const int count = (int)min((unsigned long long)tile_elems, p.n - base);
+    if (item.phase == 2 && threadIdx.x == 0) {
+      bool err = false;
+      if (item.chunk > known_ready) {
+        wait_flag(p.chunk_status + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
+        if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
+      }
+      s_carry = ld_status(p.status + tile).payload;
+    }
+    if (item.phase == 2) known_ready = max(known_ready, item.chunk);
+    cp_async_wait_1();
+    __syncthreads();
+
+    int kept;
+    const unsigned keep = thread_flags<T, ITEMS>(buf, count, p, &kept);
+    unsigned long long tile_kept;
+    const unsigned long long texcl =
+        block_exclusive_scan<CountOps>((unsigned long long)kept, s_warp, &tile_kept);
+    if (item.phase == 1) {
+      if (threadIdx.x == 0) {
+        int fin = 0;
+        if (tile != p.stall_tile) {
+          st_status(p.status + tile, tile_kept, epoch_tag | kFlagAgg);
+          __threadfence();
+          const long long S = min(p.chunk_tiles, p.ntiles - item.chunk * p.chunk_tiles);
+          fin = atomicAdd(p.counters + item.chunk, 1u) == (unsigned)(S - 1);
+        }
+        s_fin = fin;
+      }
+      __syncthreads();
+      if (s_fin) {
+        __threadfence();
+        finalize_chunk<CountOps>(p, item.chunk, epoch_tag, 0ull, s_warp, &s_bits, &s_err);
+        if (threadIdx.x == 0 && item.chunk == p.nchunks - 1 && p.num_copied)
+          *p.num_copied = ld_status(p.chunk_status + item.chunk).payload;
+      }
+    } else {
+      emit_kept<T, ITEMS>(buf, obuf, keep, (int)texcl);
+      __syncthreads();
+      const unsigned long long obase = s_carry;
+      for (int i2 = threadIdx.x; i2 < (int)tile_kept; i2 += blockDim.x)
+        out[obase + i2] = *smem_elem_ptr<T>(obuf, i2);
+    }
+    __syncthreads();
+  }
+  finish_launch(p.hdr, epoch, p.counters, p.nchunks);
 }
 
 // ---------------------------------------------------------------- host
@@ -491,31 +657,104 @@ namespace {
 
 constexpr int kMaxTileElems = 8192;
 
-bool tile_ok(size_t esize_in, size_t esize_out, int block, int items) {
+// Chunk size of the two-phase kernels (bytes of input per chunk) and how
+// many chunks phase 1 runs ahead of phase 2.  B2P_SCAN_CHUNK_MB and
+// B2P_SCAN_LOOKAHEAD override them (read once).
+size_t chunk_bytes() {
+  static const size_t v = [] {
+    const char *e = getenv("B2P_SCAN_CHUNK_MB");
+    long mb = e ? atol(e) : 16;
+    return (size_t)(mb > 0 ? mb : 16) << 20;
+  }();
+  return v;
+}
+int lookahead_chunks() {
+  static const int v = [] {
+    const char *e = getenv("B2P_SCAN_LOOKAHEAD");
+    int d = e ? atoi(e) : 2;
+    return d > 0 ? d : 2;
+  }();
+  return v;
+}
+
+// Shared memory of one block: the input tile, plus a second tile for
+// outputs whose element size differs (scan) or for the compacted elements
+// (copy_if).  A thread's row must be whole 16-byte vectors.
+size_t tile_smem(size_t esize_in, size_t esize_out, int block, int items, bool compaction) {
+  const size_t t = (size_t)block * items;
+  return t * (esize_in + ((compaction || esize_in != esize_out) ? esize_out : 0));
+}
+
+bool tile_ok(size_t esize_in, size_t esize_out, int block, int items, bool compaction = false) {
   if (block * items > kMaxTileElems) return false;
-  size_t bytes = (size_t)block * items * std::max(esize_in, esize_out);
-  return bytes <= 200 * 1024;
+  if ((items * esize_in) % 16 || (items * esize_out) % 16) return false;
+  // the two-phase kernels add a second input tile
+  return tile_smem(esize_in, esize_out, block, items, compaction) + (size_t)block * items * esize_in <=
+         200 * 1024;
+}
+
+struct Layout {
+  long long ntiles, chunk_tiles, nchunks;
+  size_t bytes;
+};
+
+Layout layout_for(size_t n, size_t esize_in, long long tile) {
+  Layout l;
+  l.ntiles = (long long)((n + tile - 1) / tile);
+  l.chunk_tiles = std::max<long long>(1, (long long)(chunk_bytes() / ((size_t)tile * esize_in)));
+  // at most kCounterSlots chunks (larger chunks for very long inputs)
+  l.chunk_tiles = std::max<long long>(l.chunk_tiles, (l.ntiles + (long long)kCounterSlots - 1) /
+                                                         (long long)kCounterSlots);
+  l.nchunks = (l.ntiles + l.chunk_tiles - 1) / l.chunk_tiles;
+  l.bytes = kScratchPrefix + (size_t)(l.ntiles + l.nchunks) * sizeof(StatusWord);
+  return l;
+}
+
+void fill_layout(ScanParams &p, const Layout &l, void *scratch) {
+  char *s = reinterpret_cast<char *>(scratch);
+  p.hdr = reinterpret_cast<ScratchHeader *>(s);
+  p.ntiles = l.ntiles;
+  p.chunk_tiles = l.chunk_tiles;
+  p.nchunks = l.nchunks;
+  p.lookahead = lookahead_chunks();
+  p.counters = reinterpret_cast<unsigned *>(s + kHeaderBytes);
+  p.status = reinterpret_cast<StatusWord *>(s + kScratchPrefix);
+  p.chunk_status = p.status + l.ntiles;
 }
 
 template <class K>
-int launch_tiles(K kernel, ScanParams &p, const LaunchConfig &lc, size_t smem, cudaStream_t st) {
+int launch_kernel(K kernel, ScanParams &p, const LaunchConfig &lc, size_t smem, long long units,
+                  cudaStream_t st) {
   const void *kfn = (const void *)kernel;
   int rc = ensure_dynamic_smem(kfn, smem);
   if (rc) return rc;
-  int grid = grid_for(lc.grid_mode, p.ntiles, 1, kfn, lc.block, smem);
+  int grid = grid_for(lc.grid_mode, units, 1, kfn, lc.block, smem);
   kernel<<<grid, lc.block, smem, st>>>(p);
   return cuda_status(cudaGetLastError());
+}
+
+template <class P, int ITEMS, bool WIDE>
+int launch_scan_kernel(ScanParams &p, const LaunchConfig &lc, size_t smem, cudaStream_t st) {
+  if (lc.grid_mode == 0)
+    return launch_kernel(scan_lookback_kernel<P, ITEMS, WIDE>, p, lc, smem, p.ntiles, st);
+  // the two-phase kernel double-buffers its input tile
+  const size_t smem2 = smem + (size_t)lc.block * ITEMS * sizeof(typename P::In);
+  return launch_kernel(scan_twophase_kernel<P, ITEMS, WIDE>, p, lc, smem2, 2 * p.ntiles, st);
 }
 
 template <class P, int ITEMS>
 int launch_scan_items(ScanParams &p, const LaunchConfig &lc, bool wide, cudaStream_t st) {
   using In = typename P::In;
   using Out = typename P::Out;
-  size_t smem = (size_t)lc.block * ITEMS * std::max(sizeof(In), sizeof(Out));
-  if constexpr (P::kCompensated) {
-    if (wide) return launch_tiles(scan_kernel<P, ITEMS, true>, p, lc, smem, st);
+  if constexpr ((ITEMS * sizeof(In)) % 16 != 0 || (ITEMS * sizeof(Out)) % 16 != 0) {
+    return B2P_ERR_INVALID_ARG;  // masked by tile_ok; never instantiated
+  } else {
+    const size_t smem = tile_smem(sizeof(In), sizeof(Out), lc.block, ITEMS, false);
+    if constexpr (P::kCompensated) {
+      if (wide) return launch_scan_kernel<P, ITEMS, true>(p, lc, smem, st);
+    }
+    return launch_scan_kernel<P, ITEMS, false>(p, lc, smem, st);
   }
-  return launch_tiles(scan_kernel<P, ITEMS, false>, p, lc, smem, st);
 }
 
 template <class P>
@@ -525,21 +764,18 @@ int launch_scan_t(int inclusive, const void *in, void *out, size_t n, const void
   using Out = typename P::Out;
   LaunchConfig lc = describe_config(config);
   if (!tile_ok(sizeof(In), sizeof(Out), lc.block, lc.items)) return B2P_ERR_INVALID_ARG;
-  const long long tile = (long long)lc.block * lc.items;
+  const Layout l = layout_for(n, sizeof(In), (long long)lc.block * lc.items);
+  if (sb < l.bytes || (reinterpret_cast<uintptr_t>(scratch) & 255)) return B2P_ERR_SCRATCH;
   ScanParams p{};
   p.in = in;
   p.out = out;
   p.n = n;
-  p.ntiles = (long long)((n + tile - 1) / tile);
-  size_t need = kHeaderBytes + (size_t)p.ntiles * sizeof(StatusWord);
-  if (sb < need || (reinterpret_cast<uintptr_t>(scratch) & 255)) return B2P_ERR_SCRATCH;
+  fill_layout(p, l, scratch);
   p.inclusive = inclusive;
   p.has_init = init != nullptr;
   if (init) memcpy(&p.init_bits, init, sizeof(Out));
   p.vec_in = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
   p.vec_out = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
-  p.hdr = reinterpret_cast<ScratchHeader *>(scratch);
-  p.status = reinterpret_cast<StatusWord *>(reinterpret_cast<char *>(scratch) + kHeaderBytes);
   p.timeout_ns = wait_timeout_ns();
   p.stall_tile = debug_stall_tile();
   const bool wide = n > (1ull << 24);
@@ -554,8 +790,8 @@ int launch_scan_t(int inclusive, const void *in, void *out, size_t n, const void
 template <int DT>
 int scan_dispatch(int op, int inclusive, const void *in, void *out, size_t n, const void *init,
                   void *scratch, size_t sb, int config, cudaStream_t st) {
-#define B2P_SCAN_CASE(OP)                                                                   \
-  case OP:                                                                                  \
+#define B2P_SCAN_CASE(OP)                                                                       \
+  case OP:                                                                                      \
     return launch_scan_t<typename PolicyOf<DT, OP>::type>(inclusive, in, out, n, init, scratch, \
                                                           sb, config, st);
   switch (op) {
@@ -578,34 +814,39 @@ int scan_dispatch(int op, int inclusive, const void *in, void *out, size_t n, co
 #undef B2P_SCAN_CASE
 }
 
+template <class T, int ITEMS>
+int launch_copy_if_items(ScanParams &p, const LaunchConfig &lc, cudaStream_t st) {
+  const size_t smem = tile_smem(sizeof(T), sizeof(T), lc.block, ITEMS, true);
+  if (lc.grid_mode == 0)
+    return launch_kernel(copy_if_lookback_kernel<T, ITEMS>, p, lc, smem, p.ntiles, st);
+  const size_t smem2 = smem + (size_t)lc.block * ITEMS * sizeof(T);
+  return launch_kernel(copy_if_twophase_kernel<T, ITEMS>, p, lc, smem2, 2 * p.ntiles, st);
+}
+
 template <class T>
 int launch_copy_if_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs,
                      uint64_t *num_copied, void *scratch, size_t sb, int config, cudaStream_t st) {
   LaunchConfig lc = describe_config(config);
-  if (!tile_ok(sizeof(T), sizeof(T), lc.block, lc.items)) return B2P_ERR_INVALID_ARG;
-  const long long tile = (long long)lc.block * lc.items;
+  if (!tile_ok(sizeof(T), sizeof(T), lc.block, lc.items, true)) return B2P_ERR_INVALID_ARG;
+  const Layout l = layout_for(n, sizeof(T), (long long)lc.block * lc.items);
+  if (sb < l.bytes || (reinterpret_cast<uintptr_t>(scratch) & 255)) return B2P_ERR_SCRATCH;
   ScanParams p{};
   p.in = in;
   p.out = out;
   p.n = n;
-  p.ntiles = (long long)((n + tile - 1) / tile);
-  size_t need = kHeaderBytes + (size_t)p.ntiles * sizeof(StatusWord);
-  if (sb < need || (reinterpret_cast<uintptr_t>(scratch) & 255)) return B2P_ERR_SCRATCH;
+  fill_layout(p, l, scratch);
   p.vec_in = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
-  p.hdr = reinterpret_cast<ScratchHeader *>(scratch);
-  p.status = reinterpret_cast<StatusWord *>(reinterpret_cast<char *>(scratch) + kHeaderBytes);
   p.timeout_ns = wait_timeout_ns();
   p.stall_tile = debug_stall_tile();
   p.mask = mask;
   p.rhs = rhs;
   p.cmp = cmp;
   p.num_copied = reinterpret_cast<unsigned long long *>(num_copied);
-  size_t smem = (size_t)lc.block * lc.items * sizeof(T);
   switch (lc.items) {
-  case 4: return launch_tiles(copy_if_kernel<T, 4>, p, lc, smem, st);
-  case 8: return launch_tiles(copy_if_kernel<T, 8>, p, lc, smem, st);
-  case 16: return launch_tiles(copy_if_kernel<T, 16>, p, lc, smem, st);
-  default: return launch_tiles(copy_if_kernel<T, 32>, p, lc, smem, st);
+  case 4: return launch_copy_if_items<T, 4>(p, lc, st);
+  case 8: return launch_copy_if_items<T, 8>(p, lc, st);
+  case 16: return launch_copy_if_items<T, 16>(p, lc, st);
+  default: return launch_copy_if_items<T, 32>(p, lc, st);
   }
 }
 
@@ -617,14 +858,26 @@ bool scan_config_valid(int dtype, int config) {
   return tile_ok(dtype_size(dtype), acc_size(dtype), lc.block, lc.items);
 }
 
+bool copy_if_config_valid(int dtype, int config) {
+  if (config < 0 || config >= B2P_NUM_CONFIGS) return false;
+  const size_t es = dtype_size(dtype);
+  if (es != 4 && es != 8) return false;
+  LaunchConfig lc = describe_config(config);
+  return tile_ok(es, es, lc.block, lc.items, true);
+}
+
 size_t scan_scratch_bytes(int dtype, size_t n, int config) {
-  long long tile = 512;  // smallest tile of the table
+  const size_t es = dtype_size(dtype);
   if (config >= 0) {
     LaunchConfig lc = describe_config(config);
-    tile = (long long)lc.block * lc.items;
+    return layout_for(n, es, (long long)lc.block * lc.items).bytes;
   }
-  (void)dtype;
-  return kHeaderBytes + (size_t)((n + tile - 1) / tile) * sizeof(StatusWord);
+  size_t m = 0;
+  for (int c = 0; c < B2P_NUM_CONFIGS; ++c) {
+    LaunchConfig lc = describe_config(c);
+    m = std::max(m, layout_for(n, es, (long long)lc.block * lc.items).bytes);
+  }
+  return m;
 }
 
 size_t copy_if_scratch_bytes(int dtype, size_t n, int config) {

@@ -5,7 +5,7 @@
 namespace b2p {
 size_t segmented_scratch_bytes(int dtype, size_t n, int64_t nseg, int config) {
   (void)dtype; (void)n; (void)nseg; (void)config;
-  return kHeaderBytes;
+  return kScratchPrefix;
 }
 bool segmented_config_valid(int dtype, int config) { (void)dtype; (void)config; return false; }
 int launch_segmented(int, int, int, int, const void *, void *, const int64_t *, int64_t, size_t,

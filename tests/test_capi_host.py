@@ -55,14 +55,19 @@ def test_config_table():
 
 def test_scratch_sizes():
     L = C.lib()
-    # reduce: header + 8 bytes per run, runs bounded (~2368..4736) for large n
+    prefix = 256 + 4 * 1024  # header + fixed arrival-counter block
+    # reduce: one 16-byte word per run; runs bounded (2368..4736) for large n
     r28 = L.b2p_scratch_bytes(C.PRIM_REDUCE, C.F32, 1 << 28, 0, C.AUTO)
-    assert 256 < r28 < 256 + 8 * 2 * 4736 + 8 * 1024
-    assert L.b2p_scratch_bytes(C.PRIM_REDUCE, C.F32, 10, 0, C.AUTO) >= 264
-    # scan: header + 16 bytes per tile of the smallest tile (512 elements)
-    assert L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, 1 << 20, 0, C.AUTO) == 256 + 16 * 2048
-    b, it, _ = C.config_describe(5)
-    assert L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, 1 << 20, 0, 5) == 256 + 16 * ((1 << 20) // (b * it))
+    assert prefix < r28 <= prefix + 16 * 4736 * 2
+    assert L.b2p_scratch_bytes(C.PRIM_REDUCE, C.F32, 10, 0, C.AUTO) == prefix + 16
+    # scan: one 16-byte word per tile and per chunk; AUTO covers the smallest tile (512)
+    n = 1 << 20
+    auto = L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, n, 0, C.AUTO)
+    assert auto >= prefix + 16 * (n // 512)
+    for c in range(48):
+        b, it, _ = C.config_describe(c)
+        got = L.b2p_scratch_bytes(C.PRIM_SCAN, C.F32, n, 0, c)
+        assert prefix + 16 * (n // (b * it)) < got <= auto
 
 
 def test_status_strings():

@@ -30,6 +30,12 @@ SCAN_CONFIGS = [0, 6, 22, 41, C.AUTO]
 FLOAT_TOL = 1e-6
 
 
+def valid(prim, code, cfgs):
+    """Configs of `cfgs` the library accepts for this primitive and dtype."""
+    L = C.lib()
+    return [c for c in cfgs if c == C.AUTO or L.b2p_config_valid(prim, code, c)]
+
+
 def to_dev(a, code, offset=0):
     """numpy -> device tensor; `offset` elements of padding in front make the
     returned view start off a 16-byte boundary."""
@@ -188,7 +194,7 @@ def test_scan_int_bit_exact(dev, code, op):
         r_exc = O.scan(code, op, False, x, init)
         for off in (0, 1):
             xd = to_dev(x, code, off)
-            for cfg in SCAN_CONFIGS:
+            for cfg in valid(C.PRIM_SCAN, code, SCAN_CONFIGS):
                 assert np.array_equal(to_np(C.scan(xd, True, op, None, config=cfg)), r_inc), (n, off, cfg)
                 assert np.array_equal(to_np(C.scan(xd, True, op, init, config=cfg)), r_inc_i), (n, off, cfg)
                 assert np.array_equal(to_np(C.scan(xd, False, op, init, config=cfg)), r_exc), (n, off, cfg)
@@ -202,7 +208,7 @@ def test_scan_float_sum_vs_fp64(dev, code):
         ref_i = O.fp64_scan(code, True, x, 0.0)
         ref_e = O.fp64_scan(code, False, x, 1.5)
         xd = to_dev(x, code)
-        for cfg in SCAN_CONFIGS:
+        for cfg in valid(C.PRIM_SCAN, code, SCAN_CONFIGS):
             gi = to_np(C.scan(xd, True, "sum", None, config=cfg)).astype(np.float64)
             ge = to_np(C.scan(xd, False, "sum", 1.5, config=cfg)).astype(np.float64)
             pos = ref_i > 0
@@ -261,7 +267,7 @@ def test_copy_if_bit_exact(dev, code):
             ref = x[keep]
             for off in (0, 1):
                 xd = to_dev(x, code, off)
-                for cfg in (0, 6, 22, C.AUTO):
+                for cfg in valid(C.PRIM_COPY_IF, code, (0, 6, 22, C.AUTO)):
                     out, cnt = C.copy_if(xd, mask, cmp, rhs, config=cfg)
                     k = int(cnt.item())
                     assert k == ref.size, (n, mask, cmp, off, cfg)

@@ -25,7 +25,8 @@ def short_timeout():
 
 
 @pytest.mark.parametrize("prim", ["scan", "copy_if"])
-def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim):
+@pytest.mark.parametrize("config", [0, 16])  # look-back kernel / two-phase kernel
+def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, config):
     L = C.lib()
     n = 512 * 200
     x = torch.arange(n, dtype=torch.int32, device="cuda")
@@ -33,16 +34,16 @@ def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim):
     L.b2p_debug_stall_tile(37)
     t0 = time.time()
     if prim == "scan":
-        C.scan(x, True, "sum", None, config=0)  # 128 x 4 = 512-element tiles
+        C.scan(x, True, "sum", None, config=config)  # 128 x 4 = 512-element tiles
     else:
-        C.copy_if(x, 1, C.CMP_EQ, 0, config=0)
+        C.copy_if(x, 1, C.CMP_EQ, 0, config=config)
     err = C.device_error(clear=True)
     dt = time.time() - t0
     L.b2p_debug_stall_tile(-1)
     assert err == C.ERR_TIMEOUT
     assert dt < 30.0
     # the same scratch and context keep working
-    y = C.scan(x, True, "sum", None, config=0)
+    y = C.scan(x, True, "sum", None, config=config)
     ref = np.cumsum(np.arange(n, dtype=np.int64)).astype(np.int32)
     assert np.array_equal(y.cpu().numpy(), ref)
     assert C.device_error(clear=True) == C.OK
