@@ -204,6 +204,16 @@ int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in,
                        const void *init, void *scratch, size_t scratch_bytes,
                        int config, b2p_stream stream);
 
+/* The per-call analogue of the two functions above, for comparison: one
+ * b2p_reduce (prim = B2P_PRIM_SEG_REDUCE) or inclusive b2p_scan
+ * (B2P_PRIM_SEG_SCAN) call per non-empty segment, issued from a host loop
+ * over HOST offsets; empty reduce segments get the identity.  This is what
+ * the reference does for a batch of segments (numeric.hpp:226-279, one
+ * call each).  scratch must fit the largest segment. */
+int b2p_segmented_per_call(int prim, int dtype, int op, const void *in, void *out,
+                           const int64_t *host_offsets, int64_t nseg, void *scratch,
+                           size_t scratch_bytes, int config, b2p_stream stream);
+
 /* Wait for `stream`, then read the sticky device error word kept in
  * `scratch` (B2P_OK or B2P_ERR_TIMEOUT); clear != 0 resets it.  Blocks the
  * host.  Stands in for the reference's asynchronous error list

@@ -83,6 +83,7 @@ def _declare(L):
         "b2p_histogram_u8": ([vp, sz, vp, i, i, vp], i),
         "b2p_segmented_reduce": ([i, i, vp, vp, i64, vp, vp, vp, sz, i, vp], i),
         "b2p_segmented_scan": ([i, i, i, vp, vp, vp, i64, vp, vp, sz, i, vp], i),
+        "b2p_segmented_per_call": ([i, i, i, vp, vp, vp, i64, vp, sz, i, vp], i),
         "b2p_device_error": ([vp, vp, i], i),
         "b2p_set_wait_timeout_ns": ([u64], u64),
         "b2p_debug_stall_tile": ([i64], None),

@@ -90,13 +90,6 @@ __global__ void fill_bits_kernel(uint32_t *p, size_t nwords, uint64_t seed, int 
   }
 }
 
-__global__ void seg_offsets_kernel(int64_t *offs, int64_t nseg, size_t total) {
-  // evenly spread boundaries; lengths are then perturbed on the host side
-  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s <= nseg;
-       s += (int64_t)gridDim.x * blockDim.x)
-    offs[s] = (int64_t)((double)total * (double)s / (double)nseg);
-}
-
 }  // namespace
 
 int tune_shape(int prim, int dtype, int op, size_t n, int64_t nseg, double cv, int reps,
@@ -176,20 +169,28 @@ int tune_shape(int prim, int dtype, int op, size_t n, int64_t nseg, double cv, i
     }
   };
   std::vector<float> t((size_t)reps);
+  const bool seg = prim == B2P_PRIM_SEG_REDUCE || prim == B2P_PRIM_SEG_SCAN;
   for (int c = 0; c < B2P_NUM_CONFIGS && rc == B2P_OK; ++c) {
     if (!b2p_config_valid(prim, dtype, c)) continue;
-    int r = run(c);  // warm-up (also catches unsupported combinations)
-    if (r == B2P_ERR_UNSUPPORTED || r == B2P_ERR_INVALID_ARG) {
-      rc = r;
-      break;
+    // segmented shapes are timed as their CUDA-graph plan launches
+    b2p_plan plan = nullptr;
+    if (seg) {
+      int r = b2p_plan_segmented(&plan, prim, dtype, op, in, out, offs, ns, n, c, (b2p_stream)st);
+      if (r != B2P_OK) {
+        rc = r;
+        break;
+      }
     }
+    auto once = [&]() { return seg ? b2p_plan_launch(plan, (b2p_stream)st) : run(c); };
+    int r = once();  // warm-up (also catches unsupported combinations)
     if (r != B2P_OK) {
+      b2p_plan_destroy(plan);
       rc = r;
       break;
     }
     for (int k = 0; k < reps; ++k) {
       cudaEventRecord(e0, st);
-      run(c);
+      once();
       cudaEventRecord(e1, st);
       if (cudaEventSynchronize(e1) != cudaSuccess) {
         rc = B2P_ERR_CUDA;
@@ -197,6 +198,7 @@ int tune_shape(int prim, int dtype, int op, size_t n, int64_t nseg, double cv, i
       }
       cudaEventElapsedTime(&t[(size_t)k], e0, e1);
     }
+    b2p_plan_destroy(plan);
     std::sort(t.begin(), t.end());
     times_ms[c] = t[(size_t)reps / 2];
   }
