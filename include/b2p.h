@@ -172,7 +172,8 @@ int b2p_scan(int dtype, int op, int inclusive, const void *in, void *out,
 /* Order-preserving compaction of the elements with (x & mask) CMP rhs.
  * Element size 4 (dtype I32/U32/F32) or 8 (I64/U64/F64); mask/rhs are
  * compared on the unsigned bit pattern.  *num_copied (device-accessible,
- * may be NULL) receives the count.
+ * may be NULL) receives the count.  `out` must have room for n elements
+ * (the count is not known before the call); writes never go past n.
  * Replaces hipsycl::algorithms::copy_if (algorithms/algorithm.hpp:178-243). */
 int b2p_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask,
                 int cmp, uint64_t rhs, uint64_t *num_copied, void *scratch,

@@ -540,8 +540,12 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
     emit_kept<T, ITEMS>(buf, obuf, keep, (int)texcl);
     __syncthreads();
     const unsigned long long obase = s_carry;
-    for (int i = threadIdx.x; i < (int)tile_kept; i += blockDim.x)
-      out[obase + i] = *smem_elem_ptr<T>(obuf, i);
+    if (obase <= p.n && tile_kept <= p.n - obase) {
+      for (int i = threadIdx.x; i < (int)tile_kept; i += blockDim.x)
+        out[obase + i] = *smem_elem_ptr<T>(obuf, i);
+    } else if (threadIdx.x == 0) {
+      record_error(p.hdr, B2P_ERR_INVALID_ARG);
+    }
     __syncthreads();
   }
   finish_launch(p.hdr, epoch, nullptr, 0);
@@ -610,7 +614,11 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
         wait_flag(p.chunk_status + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
         if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
       }
-      s_carry = ld_status(p.status + tile).payload;
+      // the offset is an output address: accept it only from this launch's
+      // prefix word (after a time-out the word may be stale)
+      const StatusWord w = ld_status(p.status + tile);
+      const bool ok = (w.meta & ~0xffull) == epoch_tag && (w.meta & kFlagPrefix);
+      s_carry = ok ? w.payload : ~0ull;
     }
     if (item.phase == 2) known_ready = max(known_ready, item.chunk);
     cp_async_wait_1();
@@ -643,8 +651,12 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
       emit_kept<T, ITEMS>(buf, obuf, keep, (int)texcl);
       __syncthreads();
       const unsigned long long obase = s_carry;
-      for (int i2 = threadIdx.x; i2 < (int)tile_kept; i2 += blockDim.x)
-        out[obase + i2] = *smem_elem_ptr<T>(obuf, i2);
+      if (obase <= p.n && tile_kept <= p.n - obase) {
+        for (int i2 = threadIdx.x; i2 < (int)tile_kept; i2 += blockDim.x)
+          out[obase + i2] = *smem_elem_ptr<T>(obuf, i2);
+      } else if (threadIdx.x == 0) {
+        record_error(p.hdr, obase == ~0ull ? B2P_ERR_TIMEOUT : B2P_ERR_INVALID_ARG);
+      }
     }
     __syncthreads();
   }
