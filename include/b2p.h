@@ -150,6 +150,32 @@ int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out,
                const void *init, void *scratch, size_t scratch_bytes,
                int config, b2p_stream stream);
 
+/* Size of the library-resident scratch area used by b2p_reduce_static,
+ * and the largest element count that entry point accepts. */
+#define B2P_STATIC_SCRATCH_BYTES (128u * 1024u)
+#define B2P_STATIC_MAX_ELEMS ((size_t)1 << 34)
+
+/* Allocation-free reduce: the same result as b2p_reduce for the same
+ * arguments, but with no scratch argument.  No counterpart in the reference
+ * (its reduce always obtains scratch from an allocation_group).
+ *
+ * For callers that cannot allocate device memory -- code running inside a
+ * device-memory allocator or pool callback, real-time paths whose memory is
+ * fixed at start-up, host runtimes that own the device heap.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine; its scratch is a
+ * B2P_STATIC_SCRATCH_BYTES array inside the library, which every GPU that
+ * loads the library keeps until the process exits.
+ *  - The first call on each device looks up that array's device address
+ *    (cudaGetSymbolAddress, with the device current); make that first call
+ *    before any stream capture.
+ *  - All calls on a device share the one array: calls that can overlap on
+ *    the GPU (different streams without ordering) race and must not be
+ *    issued.  Each call clears the array's counters before its launch.
+ *  - n > B2P_STATIC_MAX_ELEMS returns B2P_ERR_INVALID_ARG; a call whose
+ *    scratch need exceeds the array returns B2P_ERR_SCRATCH. */
+int b2p_reduce_static(int dtype, int op, const void *in, size_t n, void *out,
+                      const void *init, b2p_stream stream);
+
 /* *out = init + sum a[i]*b[i]  (transform_reduce with plus/multiplies,
  * algorithms/numeric.hpp:170-192,215-223).  dtype F32, BF16 (fp32 out) or
  * F64.  fp32 uses Dot2 (fma TwoProduct + TwoSum). */

@@ -78,6 +78,7 @@ def _declare(L):
         "b2p_scratch_init": ([vp, sz, vp], i),
         "b2p_reduce": ([i, i, vp, sz, vp, vp, vp, sz, i, vp], i),
         "b2p_dot": ([i, vp, vp, sz, vp, vp, vp, sz, i, vp], i),
+        "b2p_reduce_static": ([i, i, vp, sz, vp, vp, vp], i),
         "b2p_scan": ([i, i, i, vp, vp, sz, vp, vp, sz, i, vp], i),
         "b2p_copy_if": ([i, vp, vp, sz, u64, i, u64, vp, vp, sz, i, vp], i),
         "b2p_histogram_u8": ([vp, sz, vp, i, i, vp], i),
