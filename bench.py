@@ -184,6 +184,7 @@ def main():
         torch.cuda.synchronize()
 
     peak, peak_kind = hbm_peak()
+    selector_state = install_selector(C)
     n = N28
     a_h = C.synth_fill(1, 1 + 10 * rank, n, 0.125, 1e-6)
     b_h = C.synth_fill(1, 2 + 10 * rank, n, 0.125, 1e-6)
@@ -262,6 +263,9 @@ def main():
             result["cpu_baseline"] = cpu_baseline(a_h, b_h, x_h)
         if not args.no_ops:
             result["ops"] = measure_ops(C, torch, np, peak)
+            result["segmented"] = measure_segmented(C, torch, np, peak)
+            result["selector"] = measure_selector_stream(selector_state)
+        result["selector_state"] = selector_state["status"]
     else:
         result["e2e"] = None
     if rank == 0:
@@ -269,6 +273,87 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def install_selector(C):
+    """Install the learned schedule selector for B2P_CONFIG_AUTO when its
+    weights match this GPU and library version (else AUTO stays heuristic)."""
+    from opensycl_b200 import selector as S
+    state = {"status": "heuristic", "sel": None}
+    try:
+        sel = S.Selector(seed=1)
+        if sel.load(S.WEIGHTS):
+            sel.install()
+            state = {"status": "learned (opensycl_b200/data/selector_b200.bin)", "sel": sel}
+        else:
+            state["status"] = "heuristic (selector weights do not match this GPU/library)"
+    except Exception as e:  # no weights file
+        state["status"] = f"heuristic ({e})"
+    return state
+
+
+def measure_segmented(C, torch, np, peak):
+    """10,000 segments, lengths log-uniform in [1, 2^20] scaled to 2^28 elements
+    in total, fp32 N(0,1) and int64 U[-2^20, 2^20]: one CUDA-graph plan launch
+    (configuration from AUTO = learned selector, and from the fixed heuristic)
+    against one plain call per segment."""
+    import ctypes
+    L = C.lib()
+    nseg = 10000
+    offs = C.synth_segments(6, nseg, 20.0, 1 << 28)
+    total = int(offs[-1])
+    od = torch.from_numpy(offs).cuda()
+    s = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(s.cuda_stream)
+    res = {"nseg": nseg, "total_elems": total,
+           "lengths": {"min": int(np.diff(offs).min()), "max": int(np.diff(offs).max())}}
+    for name, kind, code, a, b, seed, es in (("fp32", 1, C.F32, 0.0, 0.0, 7, 4),
+                                             ("int64", 5, C.I64, -(1 << 20), 1 << 20, 8, 8)):
+        x = torch.from_numpy(C.synth_fill(kind, seed, total, a, b)).cuda()
+        for prim, label in ((C.PRIM_SEG_REDUCE, "reduce"), (C.PRIM_SEG_SCAN, "inclusive_scan")):
+            out = torch.empty(nseg if prim == C.PRIM_SEG_REDUCE else total, dtype=x.dtype, device="cuda")
+            nbytes = es * total * (1 if prim == C.PRIM_SEG_REDUCE else 2) + 8 * (nseg + 1)
+            entry = {"bytes": nbytes}
+            for pol, cfg in (("learned", C.AUTO),
+                             ("heuristic", L.b2p_heuristic_config(prim, code, total, nseg))):
+                plan = ctypes.c_void_p()
+                C.check(L.b2p_plan_segmented(ctypes.byref(plan), prim, code, C.SUM, x.data_ptr(), out.data_ptr(),
+                                             od.data_ptr(), nseg, total, cfg, sh), "plan")
+                ms = _time_op(torch, lambda: C.check(L.b2p_plan_launch(plan, sh)), reps=10)
+                entry[pol] = {"config": L.b2p_plan_config(plan), "ms": round(ms, 4),
+                              "batch_calls_per_s": round(1e3 / ms, 1),
+                              "GB/s": round(nbytes / (ms / 1e3) / 1e9, 1)}
+                L.b2p_plan_destroy(plan)
+            sb = L.b2p_scratch_bytes(C.PRIM_REDUCE if prim == C.PRIM_SEG_REDUCE else C.PRIM_SCAN, code,
+                                     1 << 21, 0, C.AUTO)
+            scratch = torch.zeros(sb + 512, dtype=torch.uint8, device="cuda")
+            sp = ctypes.c_void_p((scratch.data_ptr() + 255) & ~255)
+            offs_c = offs.ctypes.data_as(ctypes.c_void_p)
+            plain = lambda: C.check(L.b2p_segmented_per_call(prim, code, C.SUM, x.data_ptr(), out.data_ptr(),
+                                                            offs_c, nseg, sp, sb, C.AUTO, sh), "per-call")
+            ms_plain = _time_op(torch, plain, reps=3, warm=1)
+            entry["plain_per_segment_calls"] = {"ms": round(ms_plain, 3), "launches": nseg,
+                                                "batch_calls_per_s": round(1e3 / ms_plain, 2)}
+            entry["speedup_learned_vs_plain"] = round(ms_plain / entry["learned"]["ms"], 1)
+            entry["speedup_learned_vs_heuristic"] = round(entry["heuristic"]["ms"] / entry["learned"]["ms"], 3)
+            res[f"{label}_{name}"] = entry
+        del x
+    return res
+
+
+def measure_selector_stream(state, ncalls=20000):
+    """A seeded stream of calls (random op, dtype, n in 2^10..2^28) run end to
+    end under the learned selector, the exhaustive tuner's table and the fixed
+    heuristic (the 100,000-call version is in profiles/)."""
+    if state.get("sel") is None:
+        return {"skipped": state["status"]}
+    from opensycl_b200 import selector as S
+    shapes, X, T, _ = S.load_dataset(S.DATASET)
+    r = S.evaluate_stream(state["sel"], shapes, T, ncalls=ncalls, seed=10, regret_sample=0)
+    return {"ncalls": ncalls, "stream_ms": {k: round(v, 2) for k, v in r["stream_ms"].items()},
+            "learned_vs_exhaustive_table": round(r["learned_vs_exhaustive_table"], 4),
+            "heuristic_vs_learned": round(r["heuristic_vs_learned"], 4),
+            "calls_per_s": {k: round(v, 1) for k, v in r["calls_per_s"].items()}}
 
 
 def measure_e2e(C, torch, a_h, b_h, x_h, args):

@@ -49,7 +49,8 @@ struct ScanParams {
   int vec_out;                   // output 16-byte aligned
   ScratchHeader *hdr;
   StatusWord *status;            // one word per tile
-  StatusWord *chunk_status;      // two-phase: one word per chunk
+  StatusWord *chunk_status;      // two-phase: chunk totals / inclusive prefixes (look-back)
+  StatusWord *chunk_carry;       // two-phase: exclusive carry of each chunk
   unsigned *counters;            // two-phase: phase-1 arrivals per chunk
   long long chunk_tiles, nchunks;
   int lookahead;
@@ -201,8 +202,12 @@ __device__ __forceinline__ WorkItem decode_work(long long w, long long ntiles, l
   return it;
 }
 
-// Last block of a chunk's phase 1: turn the chunk's tile totals into
-// per-tile exclusive prefixes and publish the chunk's running total.
+// Last block of a chunk's phase 1.  (1) Turn the chunk's tile totals into
+// chunk-relative exclusive prefixes (no waiting).  (2) Publish the chunk
+// total and obtain the chunk's exclusive carry with a warp-parallel
+// look-back over the chunk totals (so chunks do not wait for each other's
+// finalisation in sequence), then publish the carry.  Phase 2 combines the
+// carry with a tile's relative prefix.
 template <class Ops>
 __device__ void finalize_chunk(const ScanParams &p, long long k, unsigned long long epoch_tag,
                                unsigned long long init_bits, typename Ops::Pub *s_pub,
@@ -210,29 +215,44 @@ __device__ void finalize_chunk(const ScanParams &p, long long k, unsigned long l
   using Pub = typename Ops::Pub;
   const long long c0 = k * p.chunk_tiles;
   const long long S = min(p.chunk_tiles, p.ntiles - c0);
-  if (threadIdx.x == 0) {
-    bool err = false;
-    *s_bits = k == 0 ? init_bits
-                     : wait_flag(p.chunk_status + (k - 1), epoch_tag, kFlagPrefix, p.timeout_ns, &err);
-    *s_err = err;
-  }
-  __syncthreads();
-  __threadfence();
-  Pub carry = Ops::unpack(*s_bits);
-  const bool err = *s_err != 0;
+  Pub rel = Ops::identity();
   for (long long b = 0; b < S; b += blockDim.x) {
     const long long i = b + threadIdx.x;
     Pub v = i < S ? Ops::unpack(ld_status(p.status + c0 + i).payload) : Ops::identity();
     Pub tot;
     Pub ex = block_exclusive_scan<Ops>(v, s_pub, &tot);
-    if (i < S) st_status(p.status + c0 + i, Ops::pack(Ops::combine(carry, ex)), epoch_tag | kFlagPrefix);
-    carry = Ops::combine(carry, tot);
+    if (i < S) st_status(p.status + c0 + i, Ops::pack(Ops::combine(rel, ex)), epoch_tag | kFlagPrefix);
+    rel = Ops::combine(rel, tot);
     __syncthreads();
   }
+  __threadfence();  // every writer: relative prefixes visible before the carry below
+  if (threadIdx.x < 32) {
+    Pub carry = Ops::unpack(init_bits);
+    bool err = false;
+    if (k == 0) {
+      if (threadIdx.x == 0)
+        st_status(p.chunk_status, Ops::pack(Ops::combine(carry, rel)), epoch_tag | kFlagPrefix);
+    } else {
+      if (threadIdx.x == 0) st_status(p.chunk_status + k, Ops::pack(rel), epoch_tag | kFlagAgg);
+      // chunk 0's prefix includes init and later chunks' totals do not, so
+      // the look-back result already counts init exactly once
+      carry = lookback<Ops>(p.chunk_status, k, epoch_tag, p.timeout_ns, err);
+    }
+    if (threadIdx.x == 0) {
+      *s_bits = Ops::pack(carry);
+      *s_err = err;
+    }
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
+    const bool err = *s_err != 0;
     if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
-    __threadfence();
-    st_status(p.chunk_status + k, Ops::pack(carry), epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
+    if (k > 0) {
+      st_status(p.chunk_status + k, Ops::pack(Ops::combine(Ops::unpack(*s_bits), rel)),
+                epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
+    }
+    __threadfence();  // relative prefixes before the carry that enables phase 2
+    st_status(p.chunk_carry + k, *s_bits, epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
   }
 }
 
@@ -343,7 +363,8 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
   const unsigned long long epoch = s_epoch;
   const unsigned long long epoch_tag = epoch << 8;
   const unsigned long long init_bits = init_value<P, WIDE>(p);
-  long long known_ready = -1;  // chunks become ready in order
+  long long known_chunk = -1;  // thread 0: chunk whose carry is in known_bits
+  unsigned long long known_bits = 0;
 
   // Bring the input tile of work id w into buf (phase-1 reads are kept in
   // L2 for phase 2; phase-2 reads release their lines).
@@ -379,14 +400,16 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
     const unsigned long long base = (unsigned long long)tile * tile_elems;
     const int count = (int)min((unsigned long long)tile_elems, p.n - base);
     if (item.phase == 2 && threadIdx.x == 0) {
-      bool err = false;
-      if (item.chunk > known_ready) {
-        wait_flag(p.chunk_status + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
+      // tile carry = chunk carry (+) chunk-relative prefix of the tile
+      if (item.chunk != known_chunk) {
+        bool err = false;
+        known_bits = wait_flag(p.chunk_carry + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
         if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        known_chunk = item.chunk;
       }
-      s_carry = ld_status(p.status + tile).payload;
+      s_carry = Ops::pack(Ops::combine(Ops::unpack(known_bits),
+                                       Ops::unpack(ld_status(p.status + tile).payload)));
     }
-    if (item.phase == 2) known_ready = max(known_ready, item.chunk);
     cp_async_wait_1();  // this item's tile has landed
     __syncthreads();
 
@@ -575,7 +598,8 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
   __syncthreads();
   const unsigned long long epoch = s_epoch;
   const unsigned long long epoch_tag = epoch << 8;
-  long long known_ready = -1;
+  long long known_chunk = -1;  // thread 0: chunk whose carry is in known_bits
+  unsigned long long known_bits = 0;
 
   auto prefetch = [&](long long w, char *buf) {
     if (w < nitems) {
@@ -609,18 +633,21 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
     const unsigned long long base = (unsigned long long)tile * tile_elems;
     const int count = (int)min((unsigned long long)tile_elems, p.n - base);
     if (item.phase == 2 && threadIdx.x == 0) {
-      bool err = false;
-      if (item.chunk > known_ready) {
-        wait_flag(p.chunk_status + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
-        if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
+      if (item.chunk != known_chunk) {
+        bool err = false;
+        known_bits = wait_flag(p.chunk_carry + item.chunk, epoch_tag, kFlagPrefix, p.timeout_ns, &err);
+        if (err) {
+          record_error(p.hdr, B2P_ERR_TIMEOUT);
+          known_bits = ~0ull;
+        }
+        known_chunk = item.chunk;
       }
       // the offset is an output address: accept it only from this launch's
-      // prefix word (after a time-out the word may be stale)
+      // words (after a time-out they may be stale)
       const StatusWord w = ld_status(p.status + tile);
-      const bool ok = (w.meta & ~0xffull) == epoch_tag && (w.meta & kFlagPrefix);
-      s_carry = ok ? w.payload : ~0ull;
+      const bool ok = known_bits != ~0ull && (w.meta & ~0xffull) == epoch_tag && (w.meta & kFlagPrefix);
+      s_carry = ok ? known_bits + w.payload : ~0ull;
     }
-    if (item.phase == 2) known_ready = max(known_ready, item.chunk);
     cp_async_wait_1();
     __syncthreads();
 
@@ -645,7 +672,7 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
         __threadfence();
         finalize_chunk<CountOps>(p, item.chunk, epoch_tag, 0ull, s_warp, &s_bits, &s_err);
         if (threadIdx.x == 0 && item.chunk == p.nchunks - 1 && p.num_copied)
-          *p.num_copied = ld_status(p.chunk_status + item.chunk).payload;
+          *p.num_copied = ld_status(p.chunk_status + item.chunk).payload;  // inclusive count
       }
     } else {
       emit_kept<T, ITEMS>(buf, obuf, keep, (int)texcl);
@@ -654,8 +681,8 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
       if (obase <= p.n && tile_kept <= p.n - obase) {
         for (int i2 = threadIdx.x; i2 < (int)tile_kept; i2 += blockDim.x)
           out[obase + i2] = *smem_elem_ptr<T>(obuf, i2);
-      } else if (threadIdx.x == 0) {
-        record_error(p.hdr, obase == ~0ull ? B2P_ERR_TIMEOUT : B2P_ERR_INVALID_ARG);
+      } else if (threadIdx.x == 0 && obase != ~0ull) {
+        record_error(p.hdr, B2P_ERR_INVALID_ARG);
       }
     }
     __syncthreads();
@@ -718,7 +745,7 @@ Layout layout_for(size_t n, size_t esize_in, long long tile) {
   l.chunk_tiles = std::max<long long>(l.chunk_tiles, (l.ntiles + (long long)kCounterSlots - 1) /
                                                          (long long)kCounterSlots);
   l.nchunks = (l.ntiles + l.chunk_tiles - 1) / l.chunk_tiles;
-  l.bytes = kScratchPrefix + (size_t)(l.ntiles + l.nchunks) * sizeof(StatusWord);
+  l.bytes = kScratchPrefix + (size_t)(l.ntiles + 2 * l.nchunks) * sizeof(StatusWord);
   return l;
 }
 
@@ -732,6 +759,7 @@ void fill_layout(ScanParams &p, const Layout &l, void *scratch) {
   p.counters = reinterpret_cast<unsigned *>(s + kHeaderBytes);
   p.status = reinterpret_cast<StatusWord *>(s + kScratchPrefix);
   p.chunk_status = p.status + l.ntiles;
+  p.chunk_carry = p.chunk_status + l.nchunks;
 }
 
 template <class K>

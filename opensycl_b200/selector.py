@@ -281,6 +281,7 @@ def evaluate_stream(sel: Selector, train_shapes, train_T, ncalls=100000, seed=10
             tk = float(t[cfgs[i]])
             regret[k].append(tk / tb - 1.0)
             best_sum[k] += tk
+    opt_sum = opt_sum or float("nan")
     return {
         "ncalls": ncalls, "seed": seed, "stream_ms": times,
         "learned_vs_exhaustive_table": times["learned"] / times["exhaustive_table"],
@@ -288,7 +289,7 @@ def evaluate_stream(sel: Selector, train_shapes, train_T, ncalls=100000, seed=10
         "calls_per_s": {k: ncalls / (v / 1e3) for k, v in times.items()},
         "predict_s_for_stream": t_predict,
         "regret_sample": len(idx),
-        "mean_regret": {k: float(np.mean(v)) for k, v in regret.items()},
+        "mean_regret": {k: (float(np.mean(v)) if v else None) for k, v in regret.items()},
         "sample_time_vs_best": {k: best_sum[k] / opt_sum for k in pol},
     }
 
