@@ -55,6 +55,14 @@ int launch_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask
                    uint64_t rhs, uint64_t *num_copied, void *scratch, size_t scratch_bytes,
                    int config, cudaStream_t s);
 bool scan_config_valid(int dtype, int config);
+
+// Pipelined (TMA) scan of grid mode 1.  Returns B2P_ERR_UNSUPPORTED, having
+// launched nothing, when the call does not fit it (bf16, a pointer not
+// 16-byte aligned, fewer elements than one tile, a tile shape without a
+// pipelined kernel); the caller then runs the two-phase kernel.
+bool scan_tma_shape(int dtype, int block, int items);
+int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
+                    const void *init, void *scratch, int block, int items, cudaStream_t s);
 bool copy_if_config_valid(int dtype, int config);
 
 // Histogram.

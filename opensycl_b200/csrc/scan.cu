@@ -29,7 +29,7 @@
 // fp32/bf16 SUM accumulates with compensated (TwoSum) arithmetic; scans
 // longer than 2^24 carry cross-tile prefixes in FP64.  All waits are bounded
 // and report B2P_ERR_TIMEOUT through the scratch error word.
-#include "tile.cuh"
+#include "scan_tile.cuh"
 #include "internal.h"
 
 #include <algorithm>
@@ -61,84 +61,6 @@ struct ScanParams {
   int cmp;
   unsigned long long *num_copied;
 };
-
-// ------------------------------------------------------- per-tile phases
-
-// Thread total of this thread's ITEMS consecutive elements of the shared
-// tile (blocked arrangement, 16-byte reads).
-template <class P, int ITEMS>
-__device__ __forceinline__ typename P::Acc thread_total(const char *buf, int count) {
-  using In = typename P::In;
-  constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
-  const int first = threadIdx.x * ITEMS;
-  typename P::Acc agg = P::identity();
-#pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&w);
-#pragma unroll
-    for (int q = 0; q < IPV; ++q)
-      if (first + k * IPV + q < count) P::add(agg, e[q]);
-  }
-  if constexpr (P::kCompensated) agg = df_norm(agg);
-  return agg;
-}
-
-// Re-read the inputs and write the outputs one 16-byte vector at a time.
-// With equal element sizes each output vector overwrites the input vector
-// it came from, which only this thread reads.
-template <class P, int ITEMS>
-__device__ __forceinline__ void emit_scan(const char *buf, char *obuf, typename P::Acc run,
-                                          bool inclusive) {
-  using In = typename P::In;
-  using Out = typename P::Out;
-  constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int OPV = 16 / (int)sizeof(Out);
-  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
-  constexpr int OUT_PER_IN = IPV / OPV;
-#pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&w);
-#pragma unroll
-    for (int m = 0; m < OUT_PER_IN; ++m) {
-      uint4 o;
-      Out *oe = reinterpret_cast<Out *>(&o);
-#pragma unroll
-      for (int q = 0; q < OPV; ++q) {
-        const In xv = e[m * OPV + q];
-        if (inclusive) {
-          P::add(run, xv);
-          oe[q] = P::finalize(run);
-        } else {
-          oe[q] = P::finalize(run);
-          P::add(run, xv);
-        }
-      }
-      *reinterpret_cast<uint4 *>(obuf + swz((threadIdx.x * VPT + k) * OUT_PER_IN + m) * 16) = o;
-    }
-  }
-}
-
-// Running value of a thread: carry (+) the thread's exclusive prefix.
-template <class P, bool WIDE>
-__device__ __forceinline__ typename P::Acc start_value(unsigned long long carry_bits,
-                                                       typename P::Acc texcl) {
-  if constexpr (WIDE) {
-    const double c = F64Ops::unpack(carry_bits) + ((double)texcl.hi + (double)texcl.lo);
-    const float h = (float)c;
-    return DF{h, (float)(c - (double)h)};
-  } else {
-    return P::combine(P::unpack(carry_bits), texcl);
-  }
-}
-
-template <class P, bool WIDE>
-__device__ __forceinline__ unsigned long long publish_value(typename P::Acc a) {
-  if constexpr (WIDE) return F64Ops::pack((double)a.hi + (double)a.lo);
-  else return P::pack(a);
-}
 
 template <class P, bool WIDE>
 __device__ __forceinline__ unsigned long long init_value(const ScanParams &p) {
@@ -926,6 +848,14 @@ size_t copy_if_scratch_bytes(int dtype, size_t n, int config) {
 
 int launch_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
                 const void *init, void *scratch, size_t sb, int config, cudaStream_t st) {
+  if (config >= 0 && config < B2P_NUM_CONFIGS) {
+    const LaunchConfig lc = describe_config(config);
+    if (lc.grid_mode == 1 && scan_tma_shape(dtype, lc.block, lc.items) &&
+        sb >= scan_scratch_bytes(dtype, n, config)) {
+      const int rc = launch_scan_tma(dtype, op, inclusive, in, out, n, init, scratch, lc.block, lc.items, st);
+      if (rc != B2P_ERR_UNSUPPORTED) return rc;
+    }
+  }
   switch (dtype) {
   case B2P_I32: return scan_dispatch<B2P_I32>(op, inclusive, in, out, n, init, scratch, sb, config, st);
   case B2P_I64: return scan_dispatch<B2P_I64>(op, inclusive, in, out, n, init, scratch, sb, config, st);

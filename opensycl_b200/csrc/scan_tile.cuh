@@ -1,0 +1,89 @@
+// Per-tile phases shared by the scan kernels: a thread's total over its
+// ITEMS consecutive elements of a swizzled shared tile, the emission of its
+// scanned outputs, and the conversions between a tile carry (accumulator or
+// FP64 for long fp32/bf16 sums) and a thread's running value.
+#pragma once
+
+#include "tile.cuh"
+
+namespace b2p {
+
+// ------------------------------------------------------- per-tile phases
+
+// Thread total of this thread's ITEMS consecutive elements of the shared
+// tile (blocked arrangement, 16-byte reads).
+template <class P, int ITEMS>
+__device__ __forceinline__ typename P::Acc thread_total(const char *buf, int count) {
+  using In = typename P::In;
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+  const int first = threadIdx.x * ITEMS;
+  typename P::Acc agg = P::identity();
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&w);
+#pragma unroll
+    for (int q = 0; q < IPV; ++q)
+      if (first + k * IPV + q < count) P::add(agg, e[q]);
+  }
+  if constexpr (P::kCompensated) agg = df_norm(agg);
+  return agg;
+}
+
+// Re-read the inputs and write the outputs one 16-byte vector at a time.
+// With equal element sizes each output vector overwrites the input vector
+// it came from, which only this thread reads.
+template <class P, int ITEMS>
+__device__ __forceinline__ void emit_scan(const char *buf, char *obuf, typename P::Acc run,
+                                          bool inclusive) {
+  using In = typename P::In;
+  using Out = typename P::Out;
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int OPV = 16 / (int)sizeof(Out);
+  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+  constexpr int OUT_PER_IN = IPV / OPV;
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&w);
+#pragma unroll
+    for (int m = 0; m < OUT_PER_IN; ++m) {
+      uint4 o;
+      Out *oe = reinterpret_cast<Out *>(&o);
+#pragma unroll
+      for (int q = 0; q < OPV; ++q) {
+        const In xv = e[m * OPV + q];
+        if (inclusive) {
+          P::add(run, xv);
+          oe[q] = P::finalize(run);
+        } else {
+          oe[q] = P::finalize(run);
+          P::add(run, xv);
+        }
+      }
+      *reinterpret_cast<uint4 *>(obuf + swz((threadIdx.x * VPT + k) * OUT_PER_IN + m) * 16) = o;
+    }
+  }
+}
+
+// Running value of a thread: carry (+) the thread's exclusive prefix.
+template <class P, bool WIDE>
+__device__ __forceinline__ typename P::Acc start_value(unsigned long long carry_bits,
+                                                       typename P::Acc texcl) {
+  if constexpr (WIDE) {
+    const double c = F64Ops::unpack(carry_bits) + ((double)texcl.hi + (double)texcl.lo);
+    const float h = (float)c;
+    return DF{h, (float)(c - (double)h)};
+  } else {
+    return P::combine(P::unpack(carry_bits), texcl);
+  }
+}
+
+template <class P, bool WIDE>
+__device__ __forceinline__ unsigned long long publish_value(typename P::Acc a) {
+  if constexpr (WIDE) return F64Ops::pack((double)a.hi + (double)a.lo);
+  else return P::pack(a);
+}
+
+}  // namespace b2p

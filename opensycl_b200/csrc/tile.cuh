@@ -179,10 +179,11 @@ __device__ __forceinline__ void record_error(ScratchHeader *hdr, unsigned code) 
 // their payloads.  Every wait is bounded by timeout_ns (%globaltimer,
 // checked every 64 polls); predecessors still missing at the deadline count
 // as broken links.  Returns the exclusive prefix; sets err when the chain is
-// broken.
+// broken.  kBackoff: sleep between polls (blocks that wait inline); a
+// dedicated look-back warp polls without sleeping.
 constexpr int kLookW = 4;
 
-template <class Ops>
+template <class Ops, bool kBackoff = true>
 __device__ typename Ops::Pub lookback(const StatusWord *status, long long tile,
                                       unsigned long long epoch_tag, unsigned long long timeout_ns,
                                       bool &err) {
@@ -233,7 +234,7 @@ __device__ typename Ops::Pub lookback(const StatusWord *status, long long tile,
         }
       }
       if (ok) break;
-      if (it >= 8) __nanosleep(it < 64 ? 32 : 256);
+      if (kBackoff && it >= 8) __nanosleep(it < 64 ? 32 : 256);
       if ((it & 63) == 63) {
         uint64_t now = __shfl_sync(0xffffffffu, globaltimer_ns(), 0);
         if (t0 == 0) {

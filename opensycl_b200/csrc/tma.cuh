@@ -1,0 +1,121 @@
+// Tensor-memory-accelerator (TMA) plumbing of the pipelined kernels: the
+// mbarrier protocol between the producer warp, the look-back warps and the
+// consumer warps of one block, 2-D bulk tensor copies between global memory
+// and 128-byte-swizzled shared tiles, bulk-store groups, and the host-side
+// encoding of a byte array as a 2-D "rows of 128 bytes" tensor.
+//
+// The 128-byte swizzle of a TMA tile places 16-byte chunk c of row r at
+// chunk c ^ (r & 7) of a 1024-byte-aligned buffer: exactly the layout swz()
+// in tile.cuh produces, so the blocked per-thread reads of the tile kernels
+// work on TMA-filled buffers unchanged and stay bank-conflict free.
+//
+// Every wait here is bounded (%globaltimer); a caller that sees a wait run
+// out records B2P_ERR_TIMEOUT and leaves its loop.
+#pragma once
+
+#include <cuda.h>
+
+#include "common.cuh"
+
+namespace b2p {
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+// Make barrier initialisation visible to the async proxy (TMA) before use.
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Arrive and announce `bytes` of TMA transactions for the current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase with the given parity to complete; false after
+// timeout_ns without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity, unsigned long long timeout_ns) {
+  if (mbar_try(b, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_try(b, parity))
+    if (globaltimer_ns() - t0 > timeout_ns) return false;
+  return true;
+}
+
+__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
+}
+
+// Global -> shared tile copy of box (x, y); completes `bytes` on *bar.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar, unsigned long long l2_policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      ".L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(l2_policy)
+      : "memory");
+}
+
+// Shared -> global tile copy of box (x, y); rows outside the tensor are
+// not written.  Tracked by the issuing thread's bulk groups.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int y, const void *src,
+                                             unsigned long long l2_policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group.L2::cache_hint"
+      " [%0, {%1, %2}], [%3], %4;" ::"l"(map),
+      "r"(x), "r"(y), "r"(smem_u32(src)), "l"(l2_policy)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until at most N of this thread's bulk groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Wait until all of this thread's bulk groups completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Order this thread's generic shared-memory writes before later async-proxy
+// (TMA) reads of them.
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Barrier over the first `count` threads of the block (named barrier `id`).
+__device__ __forceinline__ void bar_named(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Host: describe [base, base + rows * 128) as a tensor of `rows` rows of 128
+// bytes, read and written in boxes of box_rows rows with the 128-byte
+// swizzle.  base must be 16-byte aligned, 1 <= rows < 2^31, 1 <= box_rows
+// <= 256.  Returns false when the driver entry point is missing or rejects
+// the description.
+bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long rows, int box_rows);
+
+}  // namespace b2p

@@ -47,6 +47,11 @@ int heuristic_config(int prim, int dtype, size_t n, int64_t nseg) {
   case B2P_PRIM_DOT:
     return cfg(0, 1024, 32);
   case B2P_PRIM_SCAN:
+    // pipelined (TMA) kernel from 8 MiB of input on; below that the
+    // one-tile-per-block look-back kernel fills the GPU faster
+    if (dtype != B2P_BF16 && n * dtype_size(dtype) >= (8u << 20))
+      return cfg(1, 256, dtype_size(dtype) == 8 ? 16 : 32);
+    return cfg(0, 256, dtype_size(dtype) == 8 ? 16 : 32);
   case B2P_PRIM_COPY_IF:
     return cfg(0, 256, dtype_size(dtype) == 8 ? 16 : 32);
   case B2P_PRIM_HISTOGRAM:
@@ -57,7 +62,6 @@ int heuristic_config(int prim, int dtype, size_t n, int64_t nseg) {
   default:
     return 0;
   }
-  (void)n;
 }
 
 int auto_lookup(int prim, int dtype, size_t n, int64_t nseg, double cv) {

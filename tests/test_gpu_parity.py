@@ -26,7 +26,7 @@ TD = {C.I32: torch.int32, C.I64: torch.int64, C.U32: torch.uint32, C.U64: torch.
       C.F32: torch.float32, C.BF16: torch.bfloat16, C.F64: torch.float64}
 SIZES = [1, 2, 5, 127, 128, 1000, 4099, 65537, (1 << 20) + 3]
 REDUCE_CONFIGS = [0, 9, 22, 47, C.AUTO]
-SCAN_CONFIGS = [0, 6, 22, 41, C.AUTO]
+SCAN_CONFIGS = [0, 6, 19, 22, 23, 26, 41, C.AUTO]
 FLOAT_TOL = 1e-6
 
 
@@ -214,6 +214,48 @@ def test_scan_float_sum_vs_fp64(dev, code):
             pos = ref_i > 0
             assert np.max(np.abs(gi - ref_i)[pos] / ref_i[pos]) <= FLOAT_TOL, (n, cfg)
             assert np.max(np.abs(ge - ref_e) / ref_e) <= FLOAT_TOL, (n, cfg)
+
+
+# Pipelined (TMA) scan configurations: 128 x 32, 256 x 16, 256 x 32, 512 x 16.
+TMA_SCAN_CONFIGS = [19, 22, 23, 26]
+
+
+@pytest.mark.parametrize("code", [C.I32, C.I64, C.U32])
+def test_scan_pipelined_row_tails(dev, code):
+    """Sizes around tile and 128-byte-row boundaries: the last tile may be
+    partly or wholly past the complete rows that the bulk tensor copies
+    cover, and the elements after them go through plain loads and stores."""
+    rng = np.random.default_rng(550 + code)
+    es = np.dtype(NP[code]).itemsize
+    epr = 128 // es
+    for cfg in TMA_SCAN_CONFIGS:
+        blk, items = C.config_describe(cfg)[:2]
+        tile = blk * items
+        for n in [tile, tile + 1, 3 * tile - 1, 3 * tile + epr - 1, 5 * tile + 256 * epr,
+                  5 * tile + 256 * epr + 3, 7 * tile + tile // 2 + 5]:
+            x = rand_ints(rng, code, n, C.SUM)
+            init = rand_ints(rng, code, 1, C.SUM)[0]
+            xd = to_dev(x, code)
+            assert np.array_equal(to_np(C.scan(xd, True, C.SUM, None, config=cfg)),
+                                  O.scan(code, C.SUM, True, x)), (cfg, n)
+            assert np.array_equal(to_np(C.scan(xd, False, C.SUM, init, config=cfg)),
+                                  O.scan(code, C.SUM, False, x, init)), (cfg, n)
+
+
+def test_scan_pipelined_fp32_long_exclusive(dev):
+    """fp32 SUM longer than 2^24 (FP64 tile carries) through the pipelined
+    kernel, inclusive and exclusive with init."""
+    rng = np.random.default_rng(560)
+    n = (1 << 24) + 12345
+    x = rand_floats(rng, C.F32, n, positive=True)
+    ref_i = O.fp64_scan(C.F32, True, x, 0.0)
+    ref_e = O.fp64_scan(C.F32, False, x, 1.5)
+    xd = to_dev(x, C.F32)
+    for cfg in (22, 23):
+        gi = to_np(C.scan(xd, True, "sum", None, config=cfg)).astype(np.float64)
+        ge = to_np(C.scan(xd, False, "sum", 1.5, config=cfg)).astype(np.float64)
+        assert np.max(np.abs(gi - ref_i) / ref_i) <= FLOAT_TOL, cfg
+        assert np.max(np.abs(ge - ref_e) / ref_e) <= FLOAT_TOL, cfg
 
 
 @pytest.mark.parametrize("code", [C.F32, C.F64])

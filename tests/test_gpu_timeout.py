@@ -25,16 +25,18 @@ def short_timeout():
 
 
 @pytest.mark.parametrize("prim", ["scan", "copy_if"])
-@pytest.mark.parametrize("config", [0, 16])  # look-back kernel / two-phase kernel
-def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, config):
+# look-back kernel (128 x 4 tiles) / two-phase kernel (128 x 4) / pipelined
+# TMA scan (256 x 32 = 8192-element tiles; copy_if runs two-phase there)
+@pytest.mark.parametrize("config,stall", [(0, 37), (16, 37), (23, 5)])
+def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, config, stall):
     L = C.lib()
     n = 512 * 200
     x = torch.arange(n, dtype=torch.int32, device="cuda")
     C.device_error(clear=True)
-    L.b2p_debug_stall_tile(37)
+    L.b2p_debug_stall_tile(stall)
     t0 = time.time()
     if prim == "scan":
-        C.scan(x, True, "sum", None, config=config)  # 128 x 4 = 512-element tiles
+        C.scan(x, True, "sum", None, config=config)
     else:
         C.copy_if(x, 1, C.CMP_EQ, 0, config=config)
     err = C.device_error(clear=True)
