@@ -63,6 +63,11 @@ bool scan_config_valid(int dtype, int config);
 bool scan_tma_shape(int dtype, int block, int items);
 int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
                     const void *init, void *scratch, int block, int items, cudaStream_t s);
+// Pipelined copy_if of grid mode 1 (same fallback contract).
+bool copy_if_tma_shape(int dtype, int block, int items);
+int launch_copy_if_tma(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
+                       uint64_t rhs, uint64_t *num_copied, void *scratch, int block, int items,
+                       cudaStream_t s);
 bool copy_if_config_valid(int dtype, int config);
 
 // Histogram.

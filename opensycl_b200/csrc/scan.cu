@@ -367,23 +367,6 @@ __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
 
 // ------------------------------------------------------- copy_if kernels
 
-template <class T>
-__device__ __forceinline__ bool pred_bits(T v, unsigned long long mask, int cmp,
-                                          unsigned long long rhs) {
-  using U = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
-  U u;
-  memcpy(&u, &v, sizeof(T));
-  const U a = u & (U)mask, r = (U)rhs;
-  switch (cmp) {
-  case B2P_CMP_LT: return a < r;
-  case B2P_CMP_LE: return a <= r;
-  case B2P_CMP_EQ: return a == r;
-  case B2P_CMP_NE: return a != r;
-  case B2P_CMP_GE: return a >= r;
-  default: return a > r;
-  }
-}
-
 // Predicate flags of this thread's ITEMS consecutive elements.
 template <class T, int ITEMS>
 __device__ __forceinline__ unsigned thread_flags(const char *buf, int count, const ScanParams &p,
@@ -871,6 +854,15 @@ int launch_scan(int dtype, int op, int inclusive, const void *in, void *out, siz
 int launch_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
                    uint64_t rhs, uint64_t *num_copied, void *scratch, size_t sb, int config,
                    cudaStream_t st) {
+  if (config >= 0 && config < B2P_NUM_CONFIGS) {
+    const LaunchConfig lc = describe_config(config);
+    if (lc.grid_mode == 1 && copy_if_tma_shape(dtype, lc.block, lc.items) &&
+        sb >= copy_if_scratch_bytes(dtype, n, config)) {
+      const int rc = launch_copy_if_tma(dtype, in, out, n, mask, cmp, rhs, num_copied, scratch, lc.block,
+                                        lc.items, st);
+      if (rc != B2P_ERR_UNSUPPORTED) return rc;
+    }
+  }
   switch (dtype_size(dtype)) {
   case 4: return launch_copy_if_t<uint32_t>(in, out, n, mask, cmp, rhs, num_copied, scratch, sb, config, st);
   case 8: return launch_copy_if_t<unsigned long long>(in, out, n, mask, cmp, rhs, num_copied, scratch, sb, config, st);

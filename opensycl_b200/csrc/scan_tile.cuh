@@ -86,4 +86,22 @@ __device__ __forceinline__ unsigned long long publish_value(typename P::Acc a) {
   else return P::pack(a);
 }
 
+// copy_if predicate: (bits of v & mask) CMP rhs, compared as unsigned.
+template <class T>
+__device__ __forceinline__ bool pred_bits(T v, unsigned long long mask, int cmp,
+                                          unsigned long long rhs) {
+  using U = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
+  U u;
+  memcpy(&u, &v, sizeof(T));
+  const U a = u & (U)mask, r = (U)rhs;
+  switch (cmp) {
+  case B2P_CMP_LT: return a < r;
+  case B2P_CMP_LE: return a <= r;
+  case B2P_CMP_EQ: return a == r;
+  case B2P_CMP_NE: return a != r;
+  case B2P_CMP_GE: return a >= r;
+  default: return a > r;
+  }
+}
+
 }  // namespace b2p

@@ -309,11 +309,36 @@ def test_copy_if_bit_exact(dev, code):
             ref = x[keep]
             for off in (0, 1):
                 xd = to_dev(x, code, off)
-                for cfg in valid(C.PRIM_COPY_IF, code, (0, 6, 22, C.AUTO)):
+                for cfg in valid(C.PRIM_COPY_IF, code, (0, 6, 19, 22, 23, 26, C.AUTO)):
                     out, cnt = C.copy_if(xd, mask, cmp, rhs, config=cfg)
                     k = int(cnt.item())
                     assert k == ref.size, (n, mask, cmp, off, cfg)
                     assert np.array_equal(to_np(out[:k]).view(u.dtype), ref.view(u.dtype))
+
+
+@pytest.mark.parametrize("code", [C.U32, C.U64])
+def test_copy_if_pipelined_unaligned_output(dev, code):
+    """Pipelined copy_if writes the 16-byte-aligned middle of each tile's
+    output with one bulk copy and the ends with plain stores: outputs that
+    start at every 16-byte phase, sizes around tile and row boundaries."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(810 + code)
+    es = np.dtype(NP[code]).itemsize
+    for cfg in TMA_SCAN_CONFIGS:
+        blk, items = C.config_describe(cfg)[:2]
+        tile = blk * items
+        for n in [tile, 3 * tile + 5, 6 * tile + 128 // es * 7 + 1]:
+            u = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(NP[code])
+            keep = (u & 7) < 3
+            ref = u[keep]
+            xd = to_dev(u, code)
+            for shift in range(16 // es):
+                big = torch.empty(n + 4, dtype=TD[code], device="cuda")
+                out = big[shift:shift + n]
+                _, cnt = C.copy_if(xd, 7, C.CMP_LT, 3, out=out, config=cfg)
+                k = int(cnt.item())
+                assert k == ref.size, (cfg, n, shift)
+                assert np.array_equal(to_np(out[:k]), ref), (cfg, n, shift)
 
 
 def test_copy_if_oracle_u32(dev):
