@@ -152,6 +152,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ops", action="store_true", help="skip the per-primitive table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--log2n", type=int, default=28,
+                    help="elements per array of the headline step (small cases for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -185,7 +187,7 @@ def main():
 
     peak, peak_kind = hbm_peak()
     selector_state = install_selector(C)
-    n = N28
+    n = 1 << args.log2n
     a_h = C.synth_fill(1, 1 + 10 * rank, n, 0.125, 1e-6)
     b_h = C.synth_fill(1, 2 + 10 * rank, n, 0.125, 1e-6)
     x_h = C.synth_fill(2, 3 + 10 * rank, n, 0.125, 1e-6)
@@ -231,7 +233,12 @@ def main():
     from_dot = dres.item()
 
     value = step_bytes * args.steps * world / (ms / 1e3) / 1e9
-    kern = {"scan_kernel<f32,sum>": (scan_ms, 8.0 * n), "reduce_kernel<f32,dot>": (dot_ms, 8.0 * n)}
+    scan_cfg = C.lib().b2p_auto_config(C.PRIM_SCAN, C.F32, n, 0, 0.0)
+    dot_cfg = C.lib().b2p_auto_config(C.PRIM_DOT, C.F32, n, 0, 0.0)
+    scan_blk, scan_items, scan_mode = C.config_describe(scan_cfg)
+    scan_name = (f"scan_tma_kernel<f32 sum,{scan_blk}x{scan_items}>" if scan_mode == 1
+                 else f"scan_{'lookback' if scan_mode == 0 else 'twophase'}_kernel<f32 sum,{scan_blk}x{scan_items}>")
+    kern = {scan_name: (scan_ms, 8.0 * n), "reduce_kernel<f32 dot>": (dot_ms, 8.0 * n)}
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms, dom_bytes = kern[dom]
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
@@ -246,8 +253,9 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "fp32 dot(a,b) 2^28 + fp32 inclusive_scan 2^28 (config 2)",
+        "config": {"workload": f"fp32 dot(a,b) 2^{args.log2n} + fp32 inclusive_scan 2^{args.log2n}",
                    "elements": n, "step_bytes": step_bytes,
+                   "scan_config": scan_cfg, "dot_config": dot_cfg,
                    "l2": "inputs (3 GiB) larger than the 126 MB L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": roofline,
