@@ -55,13 +55,20 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, unsigned parity) {
 }
 
 // Wait for the phase with the given parity to complete; false after
-// timeout_ns without completion.
+// timeout_ns without completion.  try_wait suspends the thread for a while
+// by itself; the clock (a slow special-register read) is looked at only
+// every 32 polls, so that hundreds of waiting threads do not crowd the
+// pipe that the working threads need.
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity, unsigned long long timeout_ns) {
-  if (mbar_try(b, parity)) return true;
-  const uint64_t t0 = globaltimer_ns();
-  while (!mbar_try(b, parity))
-    if (globaltimer_ns() - t0 > timeout_ns) return false;
-  return true;
+  uint64_t t0 = 0;
+  for (unsigned k = 0;; ++k) {
+    if (mbar_try(b, parity)) return true;
+    if ((k & 31) == 31) {
+      const uint64_t now = globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > timeout_ns) return false;
+    }
+  }
 }
 
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *map) {
