@@ -1,0 +1,274 @@
+// Offloaded C++ standard parallel algorithms on the primitive path:
+// std::reduce (3 overloads), std::transform_reduce (3), std::inclusive_scan
+// (3), std::exclusive_scan (2) and std::copy_if, taking the execution policy
+// b2p_stdpar::par_unseq (AdaptiveCpp: the par_unseq overloads of
+// std/stdpar/pstl-impl/numeric.hpp:28-467 and pstl-impl/algorithm.hpp:150-187,
+// which its compiler pass substitutes for std::execution::par_unseq; here
+// the caller names the policy).
+//
+// Each calling thread owns one in-order queue and one scratch cache
+// (std/stdpar/detail/sycl_glue.hpp:60-189).  Ranges must be contiguous
+// (pointers, std::vector / std::array iterators).  Device-accessible memory
+// (device, managed, registered host) is used in place; pageable host memory
+// is staged through device buffers from the cache (copied in, and for
+// outputs copied back).  Every call here returns after its result is
+// complete -- reduce/copy_if block in the reference too
+// (std/stdpar/detail/offload.hpp:646-683); the scans do as well, because
+// without the reference's compiler-inserted synchronisation the caller may
+// read the output right away.  The offload decision is always "device"
+// (there is no host fallback); the per-operation history the reference
+// keeps for that decision (offload_heuristic_db.hpp:232-365) is recorded
+// and can be read with b2p_stdpar::offload_history().
+#pragma once
+
+#include "algorithms.hpp"
+
+#include <chrono>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace b2p_stdpar {
+
+struct par_unseq_policy {};
+inline constexpr par_unseq_policy par_unseq{};
+
+struct offload_record {
+  std::string op;
+  size_t n;
+  double seconds;
+};
+
+namespace detail {
+
+namespace alg = ::hipsycl::algorithms;
+
+struct tls_runtime {
+  b2p_sycl::queue q;
+  alg::util::allocation_cache cache{alg::util::allocation_type::device};
+  std::vector<offload_record> history;
+  static tls_runtime &get() {
+    thread_local tls_runtime rt;
+    return rt;
+  }
+};
+
+template <class It>
+auto raw(It it) {
+  return &*it;
+}
+
+// A device view of a contiguous range: the original pointer when the GPU
+// can reach it, otherwise a staged device copy (copied back by copy_back()).
+template <class T>
+class view {
+ public:
+  view(alg::util::allocation_group &g, tls_runtime &rt, T *p, size_t n, bool copy_in)
+      : host_(p), n_(n), rt_(rt) {
+    if (alg::detail::device_accessible(p)) {
+      dev_ = p;
+    } else {
+      dev_ = g.obtain<std::remove_cv_t<T>>(n ? n : 1);
+      if (copy_in && n)
+        rt.q.memcpy(const_cast<std::remove_cv_t<T> *>(dev_), p, n * sizeof(T));
+    }
+  }
+  T *get() const { return dev_; }
+  void copy_back(size_t count) {
+    if (dev_ != host_ && count) rt_.q.memcpy(const_cast<std::remove_cv_t<T> *>(host_), dev_, count * sizeof(T));
+  }
+
+ private:
+  T *host_;
+  T *dev_ = nullptr;
+  size_t n_;
+  tls_runtime &rt_;
+};
+
+class timer {
+ public:
+  timer(const char *op, size_t n) : op_(op), n_(n), t0_(std::chrono::steady_clock::now()) {}
+  ~timer() {
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+    tls_runtime::get().history.push_back({op_, n_, s});
+  }
+
+ private:
+  const char *op_;
+  size_t n_;
+  std::chrono::steady_clock::time_point t0_;
+};
+
+template <class T, class F>
+T reduce_impl(const char *name, size_t n, F &&launch) {
+  timer tm(name, n);
+  auto &rt = tls_runtime::get();
+  alg::util::allocation_group g(&rt.cache, rt.q.get_device());
+  T *d_out = g.obtain<T>(1);
+  launch(g, rt, d_out);
+  T r;
+  rt.q.memcpy(&r, d_out, sizeof(T));
+  rt.q.wait();
+  return r;
+}
+
+}  // namespace detail
+
+// Offload history of the calling thread: operation, size, seconds.
+inline const std::vector<offload_record> &offload_history() { return detail::tls_runtime::get().history; }
+
+}  // namespace b2p_stdpar
+
+namespace std {
+
+// ----------------------------------------------------------------- reduce
+
+template <class ForwardIt, class T, class BinaryOp>
+T reduce(const b2p_stdpar::par_unseq_policy &, ForwardIt first, ForwardIt last, T init, BinaryOp op) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return init;
+  return d::reduce_impl<T>("reduce", n, [&](auto &g, auto &rt, T *out) {
+    using V = typename std::iterator_traits<ForwardIt>::value_type;
+    d::view<const V> in(g, rt, d::raw(first), n, true);
+    hipsycl::algorithms::reduce(rt.q, g, in.get(), in.get() + n, out, init, op);
+  });
+}
+
+template <class ForwardIt, class T>
+T reduce(const b2p_stdpar::par_unseq_policy &p, ForwardIt first, ForwardIt last, T init) {
+  return std::reduce(p, first, last, init, std::plus<>{});
+}
+
+template <class ForwardIt>
+typename std::iterator_traits<ForwardIt>::value_type reduce(const b2p_stdpar::par_unseq_policy &p, ForwardIt first,
+                                                             ForwardIt last) {
+  using V = typename std::iterator_traits<ForwardIt>::value_type;
+  return std::reduce(p, first, last, V{}, std::plus<>{});
+}
+
+// ------------------------------------------------------- transform_reduce
+
+template <class ForwardIt1, class ForwardIt2, class T, class BinaryReductionOp, class BinaryTransformOp>
+T transform_reduce(const b2p_stdpar::par_unseq_policy &, ForwardIt1 first1, ForwardIt1 last1, ForwardIt2 first2,
+                   T init, BinaryReductionOp reduce, BinaryTransformOp transform) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first1, last1);
+  if (n == 0) return init;
+  return d::reduce_impl<T>("transform_reduce", n, [&](auto &g, auto &rt, T *out) {
+    using V1 = typename std::iterator_traits<ForwardIt1>::value_type;
+    using V2 = typename std::iterator_traits<ForwardIt2>::value_type;
+    d::view<const V1> a(g, rt, d::raw(first1), n, true);
+    d::view<const V2> b(g, rt, d::raw(first2), n, true);
+    hipsycl::algorithms::transform_reduce(rt.q, g, a.get(), a.get() + n, b.get(), out, init, reduce, transform);
+  });
+}
+
+template <class ForwardIt1, class ForwardIt2, class T>
+T transform_reduce(const b2p_stdpar::par_unseq_policy &p, ForwardIt1 first1, ForwardIt1 last1, ForwardIt2 first2,
+                   T init) {
+  return std::transform_reduce(p, first1, last1, first2, init, std::plus<T>{}, std::multiplies<T>{});
+}
+
+template <class ForwardIt, class T, class BinaryReductionOp, class UnaryTransformOp>
+T transform_reduce(const b2p_stdpar::par_unseq_policy &, ForwardIt first, ForwardIt last, T init,
+                   BinaryReductionOp reduce, UnaryTransformOp transform) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return init;
+  return d::reduce_impl<T>("transform_reduce", n, [&](auto &g, auto &rt, T *out) {
+    using V = typename std::iterator_traits<ForwardIt>::value_type;
+    d::view<const V> in(g, rt, d::raw(first), n, true);
+    hipsycl::algorithms::transform_reduce(rt.q, g, in.get(), in.get() + n, out, init, reduce, transform);
+  });
+}
+
+// ------------------------------------------------------------------ scans
+
+namespace b2p_stdpar_detail {
+template <bool INCL, class InputIt, class OutputIt, class Run>
+OutputIt scan_call(const char *name, InputIt first, InputIt last, OutputIt d_first, Run run) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return d_first;
+  d::timer tm(name, n);
+  auto &rt = d::tls_runtime::get();
+  hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
+  using V = typename std::iterator_traits<InputIt>::value_type;
+  using O = std::remove_reference_t<decltype(*d_first)>;
+  d::view<const V> in(g, rt, d::raw(first), n, true);
+  d::view<O> out(g, rt, d::raw(d_first), n, false);
+  run(rt.q, g, in.get(), in.get() + n, out.get());
+  out.copy_back(n);
+  rt.q.wait();
+  return d_first + n;
+}
+}  // namespace b2p_stdpar_detail
+
+template <class InputIt, class OutputIt>
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first) {
+  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first, [](auto &q, auto &g, auto a,
+                                                                                        auto b, auto o) {
+    hipsycl::algorithms::inclusive_scan(q, g, a, b, o);
+  });
+}
+
+template <class InputIt, class OutputIt, class BinaryOp>
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first,
+                        BinaryOp op) {
+  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first, [op](auto &q, auto &g, auto a,
+                                                                                          auto b, auto o) {
+    hipsycl::algorithms::inclusive_scan(q, g, a, b, o, op);
+  });
+}
+
+template <class InputIt, class OutputIt, class BinaryOp, class T>
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first,
+                        BinaryOp op, T init) {
+  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first,
+                                            [op, init](auto &q, auto &g, auto a, auto b, auto o) {
+                                              hipsycl::algorithms::inclusive_scan(q, g, a, b, o, op, init);
+                                            });
+}
+
+template <class InputIt, class OutputIt, class T, class BinaryOp>
+OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first, T init,
+                        BinaryOp op) {
+  return b2p_stdpar_detail::scan_call<false>("exclusive_scan", first, last, d_first,
+                                             [op, init](auto &q, auto &g, auto a, auto b, auto o) {
+                                               hipsycl::algorithms::exclusive_scan(q, g, a, b, o, init, op);
+                                             });
+}
+
+template <class InputIt, class OutputIt, class T>
+OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &p, InputIt first, InputIt last, OutputIt d_first,
+                        T init) {
+  return std::exclusive_scan(p, first, last, d_first, init, std::plus<>{});
+}
+
+// ---------------------------------------------------------------- copy_if
+
+template <class ForwardIt1, class ForwardIt2, class UnaryPredicate>
+ForwardIt2 copy_if(const b2p_stdpar::par_unseq_policy &, ForwardIt1 first, ForwardIt1 last, ForwardIt2 d_first,
+                   UnaryPredicate pred) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return d_first;
+  d::timer tm("copy_if", n);
+  auto &rt = d::tls_runtime::get();
+  hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
+  using V = typename std::iterator_traits<ForwardIt1>::value_type;
+  using O = std::remove_reference_t<decltype(*d_first)>;
+  d::view<const V> in(g, rt, d::raw(first), n, true);
+  d::view<O> out(g, rt, d::raw(d_first), n, false);
+  size_t *d_count = g.obtain<size_t>(1);
+  hipsycl::algorithms::copy_if(rt.q, g, in.get(), in.get() + n, out.get(), pred, d_count);
+  size_t count = 0;
+  rt.q.memcpy(&count, d_count, sizeof(size_t));
+  rt.q.wait();
+  out.copy_back(count);
+  rt.q.wait();
+  return d_first + count;
+}
+
+}  // namespace std

@@ -1,0 +1,445 @@
+// C++ drop-in layer tests (compiled with nvcc, run on one GPU): the
+// algorithms library signatures, sycl::reduction in parallel_for, group
+// algorithms, atomic_ref and the stdpar overloads.  The cases follow the
+// reference's own tests (tests/pstl/{reduce,transform_reduce,
+// inclusive_scan,exclusive_scan,copy_if}.cpp, tests/sycl/reduction.cpp,
+// tests/sycl/group_functions/group_functions_{reduce,scan}.cpp,
+// tests/sycl/atomic.cpp); expected values are computed here on the host.
+// Prints one line per failure and "ALL PASSED <n>" at the end; exit code 0
+// only when every check passed.
+#include <hipSYCL_b2p/stdpar.hpp>
+
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+#include <vector>
+
+namespace alg = hipsycl::algorithms;
+
+static int g_checks = 0, g_fail = 0;
+#define CHECK(cond, ...)                         \
+  do {                                           \
+    ++g_checks;                                  \
+    if (!(cond)) {                               \
+      ++g_fail;                                  \
+      std::printf("FAIL %s:%d: ", __FILE__, __LINE__); \
+      std::printf(__VA_ARGS__);                  \
+      std::printf("\n");                         \
+    }                                            \
+  } while (0)
+
+template <class T>
+static std::vector<T> from_dev(sycl::queue &q, const T *d, size_t n) {
+  std::vector<T> h(n);
+  if (n) q.memcpy(h.data(), d, n * sizeof(T)).wait();
+  return h;
+}
+template <class T>
+static T *to_dev(sycl::queue &q, const std::vector<T> &h) {
+  T *d = sycl::malloc_device<T>(h.size() ? h.size() : 1, q);
+  if (!h.empty()) q.memcpy(d, h.data(), h.size() * sizeof(T)).wait();
+  return d;
+}
+
+// ------------------------------------------------------ algorithms library
+
+static void test_algorithms(sycl::queue &q) {
+  alg::util::allocation_cache cache{alg::util::allocation_type::device};
+  for (size_t n : {0ul, 1ul, 127ul, 1000ul, 1000000ul}) {
+    std::vector<int> h(n);
+    std::iota(h.begin(), h.end(), 0);
+    int *d = to_dev(q, h);
+    int *out = sycl::malloc_shared<int>(1, q);
+    *out = -7;
+    {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      alg::reduce(q, g, d, d + n, out, 10).wait();
+      const long long ref = 10 + (long long)n * (n ? n - 1 : 0) / 2;
+      if (n == 0) CHECK(*out == -7, "reduce n=0 touched *out");
+      else CHECK(*out == (int)ref, "reduce iota n=%zu got %d want %lld", n, *out, ref);
+    }
+    {
+      // user operator (generic kernels)
+      alg::util::allocation_group g{&cache, q.get_device()};
+      auto op = [] __host__ __device__(int a, int b) { return a > b ? a : b; };
+      if (n) {
+        alg::reduce(q, g, d, d + n, out, -1, op).wait();
+        CHECK(*out == (int)n - 1, "reduce max lambda n=%zu got %d", n, *out);
+      }
+    }
+    {
+      // transform_reduce, unary transform (generic) and dot form on doubles
+      alg::util::allocation_group g{&cache, q.get_device()};
+      if (n) {
+        long long *lo = sycl::malloc_shared<long long>(1, q);
+        alg::transform_reduce(q, g, d, d + n, lo, 0ll, std::plus<long long>{},
+                              [] __host__ __device__(int x) { return (long long)x * 2; })
+            .wait();
+        CHECK(*lo == (long long)n * (n - 1), "transform_reduce n=%zu got %lld", n, *lo);
+        sycl::free(lo, q);
+        std::vector<double> a(n), b(n);
+        double ref = 0.5;
+        for (size_t i = 0; i < n; ++i) {
+          a[i] = (double)(i % 17) * 0.25;
+          b[i] = 1.0 + (double)(i % 5);
+          ref += a[i] * b[i];
+        }
+        double *da = to_dev(q, a), *db = to_dev(q, b), *dd = sycl::malloc_shared<double>(1, q);
+        alg::transform_reduce(q, g, da, da + n, db, dd, 0.5).wait();
+        CHECK(std::fabs(*dd - ref) <= 1e-9 * std::fabs(ref), "dot n=%zu got %.17g want %.17g", n, *dd, ref);
+        sycl::free(da, q);
+        sycl::free(db, q);
+        sycl::free(dd, q);
+      }
+    }
+    sycl::free(out, q);
+    sycl::free(d, q);
+  }
+
+  // scans: iota and multiplies with init 3 (tests/pstl/inclusive_scan.cpp)
+  for (size_t n : {0ul, 1ul, 127ul, 1000ul, 1ul << 20}) {
+    std::vector<int> h(n);
+    std::iota(h.begin(), h.end(), 0);
+    int *d = to_dev(q, h);
+    int *o = sycl::malloc_device<int>(n ? n : 1, q);
+    alg::util::allocation_group g{&cache, q.get_device()};
+    alg::inclusive_scan(q, g, d, d + n, o).wait();
+    auto got = from_dev(q, o, n);
+    std::vector<int> ref(n);
+    std::inclusive_scan(h.begin(), h.end(), ref.begin());
+    CHECK(got == ref, "inclusive_scan iota n=%zu", n);
+    alg::exclusive_scan(q, g, d, d + n, o, 3).wait();
+    got = from_dev(q, o, n);
+    std::exclusive_scan(h.begin(), h.end(), ref.begin(), 3);
+    CHECK(got == ref, "exclusive_scan iota init 3 n=%zu", n);
+    std::vector<unsigned> hu(n);
+    for (size_t i = 0; i < n; ++i) hu[i] = 1u + (unsigned)(i % 3);
+    unsigned *du = to_dev(q, hu), *ou = sycl::malloc_device<unsigned>(n ? n : 1, q);
+    alg::inclusive_scan(q, g, du, du + n, ou, std::multiplies<unsigned>{}, 3u).wait();
+    auto gotu = from_dev(q, ou, n);
+    std::vector<unsigned> refu(n);
+    std::inclusive_scan(hu.begin(), hu.end(), refu.begin(), std::multiplies<unsigned>{}, 3u);
+    CHECK(gotu == refu, "inclusive_scan multiplies init 3 n=%zu", n);
+    // user operator with transform (generic kernels)
+    alg::transform_exclusive_scan(q, g, du, du + n, ou, 5u, std::plus<unsigned>{},
+                                  [] __host__ __device__(unsigned x) { return x * x; })
+        .wait();
+    gotu = from_dev(q, ou, n);
+    std::transform_exclusive_scan(hu.begin(), hu.end(), refu.begin(), 5u, std::plus<unsigned>{},
+                                  [](unsigned x) { return x * x; });
+    CHECK(gotu == refu, "transform_exclusive_scan n=%zu", n);
+    sycl::free(d, q);
+    sycl::free(o, q);
+    sycl::free(du, q);
+    sycl::free(ou, q);
+  }
+
+  // copy_if: even predicate on none / all / half (tests/pstl/copy_if.cpp)
+  for (int mode = 0; mode < 3; ++mode) {
+    const size_t n = 1000;
+    std::vector<int> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = mode == 0 ? 2 * (int)i + 1 : mode == 1 ? 2 * (int)i : (int)i;
+    int *d = to_dev(q, h), *o = sycl::malloc_device<int>(n, q);
+    size_t *cnt = sycl::malloc_shared<size_t>(1, q);
+    alg::util::allocation_group g{&cache, q.get_device()};
+    alg::copy_if(q, g, d, d + n, o, [] __host__ __device__(int x) { return x % 2 == 0; }, cnt).wait();
+    std::vector<int> ref;
+    for (int x : h)
+      if (x % 2 == 0) ref.push_back(x);
+    CHECK(*cnt == ref.size(), "copy_if lambda mode %d count %zu want %zu", mode, *cnt, ref.size());
+    auto got = from_dev(q, o, ref.size());
+    CHECK(got == ref, "copy_if lambda mode %d values", mode);
+    // the same through the libb2p fast path predicate
+    alg::copy_if(q, g, d, d + n, o, alg::mask_compare<int>{1, 0, B2P_CMP_EQ}, cnt).wait();
+    CHECK(*cnt == ref.size(), "copy_if mask_compare mode %d count %zu", mode, *cnt);
+    got = from_dev(q, o, ref.size());
+    CHECK(got == ref, "copy_if mask_compare mode %d values", mode);
+    sycl::free(d, q);
+    sycl::free(o, q);
+    sycl::free(cnt, q);
+  }
+
+  // empty input: completed event, count 0, even with a pending dependency
+  {
+    alg::util::allocation_group g{&cache, q.get_device()};
+    size_t cnt = 99;
+    int *nothing = nullptr;
+    auto ev = alg::copy_if(q, g, nothing, nothing, nothing, [] __host__ __device__(int) { return true; }, &cnt);
+    CHECK(cnt == 0 && ev.is_complete(), "copy_if empty");
+  }
+  // the cache reuses its allocations
+  {
+    int *d = to_dev(q, std::vector<int>(5000, 1));
+    int *o = sycl::malloc_shared<int>(1, q);
+    for (int r = 0; r < 3; ++r) {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      alg::reduce(q, g, d, d + 5000, o, 0).wait();
+      CHECK(*o == 5000, "repeated reduce %d got %d", r, *o);
+    }
+    sycl::free(d, q);
+    sycl::free(o, q);
+  }
+}
+
+// ------------------------------------------------------- sycl::reduction
+
+static void test_reduction(sycl::queue &q) {
+  // tests/sycl/reduction.cpp: sums and maxima over iota
+  for (size_t n : {20ul, 128ul, 1000ul, 1024ul, 16384ul, 262144ul}) {
+    std::vector<int> h(n);
+    std::iota(h.begin(), h.end(), 0);
+    int *d = to_dev(q, h);
+    int *sum = sycl::malloc_shared<int>(1, q), *mx = sycl::malloc_shared<int>(1, q);
+    *sum = 0;
+    *mx = 0;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<int>{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; })
+        .wait();
+    q.submit([&](sycl::handler &cgh) {
+       cgh.parallel_for(sycl::range<1>(n), sycl::reduction(mx, sycl::maximum<int>{}),
+                        [=] __device__(sycl::id<1> i, auto &r) { r.combine(d[i[0]]); });
+     }).wait();
+    const long long ref = (long long)n * (n - 1) / 2;
+    CHECK(*sum == (int)ref, "reduction sum n=%zu got %d", n, *sum);
+    CHECK(*mx == (int)n - 1, "reduction max n=%zu got %d", n, *mx);
+    // without initialize_to_identity the old value takes part; with it not
+    *sum = 100;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<int>{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; })
+        .wait();
+    CHECK(*sum == (int)(ref + 100), "reduction combine-with-old n=%zu got %d", n, *sum);
+    *sum = 100;
+    q.parallel_for(sycl::range<1>(n),
+                   sycl::reduction(sum, sycl::plus<int>{}, sycl::property::reduction::initialize_to_identity{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; })
+        .wait();
+    CHECK(*sum == (int)ref, "reduction initialize_to_identity n=%zu got %d", n, *sum);
+    // float sum, tolerance 1e-3 relative (reduction.cpp uses 0.001)
+    float *fs = sycl::malloc_shared<float>(1, q);
+    *fs = 0.f;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(fs, sycl::plus<float>{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += (float)(d[i[0]] % 7) * 0.5f; })
+        .wait();
+    double fref = 0;
+    for (size_t i = 0; i < n; ++i) fref += (double)(h[i] % 7) * 0.5;
+    CHECK(std::fabs(*fs - fref) <= 1e-3 * fref, "reduction float n=%zu got %g want %g", n, *fs, fref);
+    // user operator without a known identity, explicit identity
+    auto op = [] __host__ __device__(int a, int b) { return a < b ? a : b; };
+    *mx = 5;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(mx, op),
+                   [=] __device__(sycl::id<1> i, auto &r) { r.combine(d[i[0]] + 3); })
+        .wait();
+    CHECK(*mx == 3, "reduction unknown identity n=%zu got %d", n, *mx);
+    *mx = 1000000;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(mx, 1 << 30, op),
+                   [=] __device__(sycl::id<1> i, auto &r) { r.combine(d[i[0]] + 9); })
+        .wait();
+    CHECK(*mx == 9, "reduction given identity n=%zu got %d", n, *mx);
+    sycl::free(fs, q);
+    sycl::free(sum, q);
+    sycl::free(mx, q);
+    sycl::free(d, q);
+  }
+}
+
+// ---------------------------------------------------------- group functions
+
+static void test_group_functions(sycl::queue &q) {
+  for (size_t wg : {25ul, 144ul, 256ul}) {
+    const size_t groups = 7, n = wg * groups;
+    std::vector<int> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = (int)((i * 37) % 101) - 50;
+    int *d = to_dev(q, h);
+    int *red = sycl::malloc_device<int>(n, q), *inc = sycl::malloc_device<int>(n, q),
+        *exc = sycl::malloc_device<int>(n, q), *sred = sycl::malloc_device<int>(n, q),
+        *sinc = sycl::malloc_device<int>(n, q), *sexc = sycl::malloc_device<int>(n, q);
+    q.parallel_for(sycl::nd_range<1>(sycl::range<1>(n), sycl::range<1>(wg)), [=] __device__(sycl::nd_item<1> it) {
+       const size_t i = it.get_global_id(0);
+       auto g = it.get_group();
+       auto sg = it.get_sub_group();
+       red[i] = sycl::reduce_over_group(g, d[i], sycl::plus<int>{});
+       inc[i] = sycl::inclusive_scan_over_group(g, d[i], sycl::plus<int>{});
+       exc[i] = sycl::exclusive_scan_over_group(g, d[i], 10, sycl::plus<int>{});
+       sred[i] = sycl::reduce_over_group(sg, d[i], sycl::maximum<int>{});
+       sinc[i] = sycl::inclusive_scan_over_group(sg, d[i], sycl::plus<int>{});
+       sexc[i] = sycl::exclusive_scan_over_group(sg, d[i], sycl::plus<int>{});
+     }).wait();
+    auto r = from_dev(q, red, n), a = from_dev(q, inc, n), e = from_dev(q, exc, n), sr = from_dev(q, sred, n),
+         si = from_dev(q, sinc, n), se = from_dev(q, sexc, n);
+    bool ok_r = true, ok_i = true, ok_e = true, ok_sr = true, ok_si = true, ok_se = true;
+    for (size_t gi = 0; gi < groups; ++gi) {
+      int tot = 0, run = 0;
+      for (size_t l = 0; l < wg; ++l) tot += h[gi * wg + l];
+      for (size_t l = 0; l < wg; ++l) {
+        const size_t i = gi * wg + l;
+        ok_r &= r[i] == tot;
+        ok_e &= e[i] == 10 + run;
+        run += h[i];
+        ok_i &= a[i] == run;
+      }
+      for (size_t s0 = 0; s0 < wg; s0 += 32) {
+        const size_t s1 = std::min(wg, s0 + 32);
+        int mxv = h[gi * wg + s0], srun = 0;
+        for (size_t l = s0; l < s1; ++l) mxv = std::max(mxv, h[gi * wg + l]);
+        for (size_t l = s0; l < s1; ++l) {
+          const size_t i = gi * wg + l;
+          ok_sr &= sr[i] == mxv;
+          ok_se &= se[i] == srun;
+          srun += h[i];
+          ok_si &= si[i] == srun;
+        }
+      }
+    }
+    CHECK(ok_r, "reduce_over_group wg=%zu", wg);
+    CHECK(ok_i, "inclusive_scan_over_group wg=%zu", wg);
+    CHECK(ok_e, "exclusive_scan_over_group wg=%zu", wg);
+    CHECK(ok_sr, "reduce_over_group(sub_group) wg=%zu", wg);
+    CHECK(ok_si, "inclusive_scan_over_group(sub_group) wg=%zu", wg);
+    CHECK(ok_se, "exclusive_scan_over_group(sub_group) wg=%zu", wg);
+
+    // joint algorithms: each group works on its own span of 3*wg+5 elements
+    const size_t span = 3 * wg + 5, m = span * groups;
+    std::vector<int> hj(m);
+    for (size_t i = 0; i < m; ++i) hj[i] = (int)((i * 13) % 29) - 14;
+    int *dj = to_dev(q, hj);
+    int *jr = sycl::malloc_device<int>(groups, q), *ji = sycl::malloc_device<int>(m, q),
+        *je = sycl::malloc_device<int>(m, q);
+    q.parallel_for(sycl::nd_range<1>(sycl::range<1>(n), sycl::range<1>(wg)), [=] __device__(sycl::nd_item<1> it) {
+       auto g = it.get_group();
+       const size_t gi = it.get_group(0);
+       const int *f = dj + gi * span;
+       const int v = sycl::joint_reduce(g, f, f + span, 7, sycl::plus<int>{});
+       if (it.get_local_id(0) == 0) jr[gi] = v;
+       sycl::joint_inclusive_scan(g, f, f + span, ji + gi * span, sycl::plus<int>{});
+       sycl::joint_exclusive_scan(g, f, f + span, je + gi * span, 2, sycl::plus<int>{});
+     }).wait();
+    auto hjr = from_dev(q, jr, groups), hji = from_dev(q, ji, m), hje = from_dev(q, je, m);
+    bool ok_jr = true, ok_ji = true, ok_je = true;
+    for (size_t gi = 0; gi < groups; ++gi) {
+      int tot = 7, run = 0;
+      for (size_t l = 0; l < span; ++l) tot += hj[gi * span + l];
+      ok_jr &= hjr[gi] == tot;
+      for (size_t l = 0; l < span; ++l) {
+        const size_t i = gi * span + l;
+        ok_je &= hje[i] == 2 + run;
+        run += hj[i];
+        ok_ji &= hji[i] == run;
+      }
+    }
+    CHECK(ok_jr, "joint_reduce wg=%zu", wg);
+    CHECK(ok_ji, "joint_inclusive_scan wg=%zu", wg);
+    CHECK(ok_je, "joint_exclusive_scan wg=%zu", wg);
+    for (int *p : {d, red, inc, exc, sred, sinc, sexc, dj, jr, ji, je}) sycl::free(p, q);
+  }
+}
+
+// ---------------------------------------------------------------- atomics
+
+static void test_atomics(sycl::queue &q) {
+  // fetch_add from 2048 work-items (tests/sycl/atomic.cpp)
+  unsigned *c = sycl::malloc_shared<unsigned>(4, q);
+  for (int i = 0; i < 4; ++i) c[i] = 0;
+  double *fd = sycl::malloc_shared<double>(1, q);
+  *fd = 0;
+  q.parallel_for(sycl::range<1>(2048), [=] __host__ __device__(sycl::id<1> i) {
+     sycl::atomic_ref<unsigned, sycl::memory_order::relaxed, sycl::memory_scope::device> a(c[0]);
+     a.fetch_add(1u);
+     sycl::atomic_ref<unsigned, sycl::memory_order::relaxed, sycl::memory_scope::device> m(c[1]);
+     m.fetch_max((unsigned)i[0]);
+     sycl::atomic_ref<unsigned, sycl::memory_order::acq_rel, sycl::memory_scope::device> o(c[2]);
+     o.fetch_or(1u << (i[0] % 32));
+     sycl::atomic_ref<double, sycl::memory_order::relaxed, sycl::memory_scope::device> f(*fd);
+     f.fetch_add(0.5);
+   }).wait();
+  CHECK(c[0] == 2048u, "atomic fetch_add got %u", c[0]);
+  CHECK(c[1] == 2047u, "atomic fetch_max got %u", c[1]);
+  CHECK(c[2] == 0xffffffffu, "atomic fetch_or got %x", c[2]);
+  CHECK(*fd == 1024.0, "atomic double fetch_add got %g", *fd);
+  // 256-bin histogram of uint8 keys with atomic_ref<unsigned>::fetch_add
+  const size_t n = 1 << 20;
+  std::vector<unsigned char> keys(n);
+  for (size_t i = 0; i < n; ++i) keys[i] = (unsigned char)((i * 2654435761u) >> 13);
+  unsigned char *dk = to_dev(q, keys);
+  unsigned *bins = sycl::malloc_device<unsigned>(256, q);
+  q.memset(bins, 0, 256 * sizeof(unsigned)).wait();
+  q.parallel_for(sycl::range<1>(n), [=] __host__ __device__(sycl::id<1> i) {
+     sycl::atomic_ref<unsigned, sycl::memory_order::relaxed, sycl::memory_scope::device> b(bins[dk[i[0]]]);
+     b.fetch_add(1u);
+   }).wait();
+  auto hb = from_dev(q, bins, 256);
+  std::vector<unsigned> ref(256, 0);
+  for (auto k : keys) ++ref[k];
+  CHECK(hb == ref, "atomic_ref histogram");
+  sycl::free(c, q);
+  sycl::free(fd, q);
+  sycl::free(dk, q);
+  sycl::free(bins, q);
+}
+
+// ------------------------------------------------------------------ stdpar
+
+static void test_stdpar() {
+  const auto &pol = b2p_stdpar::par_unseq;
+  for (size_t n : {0ul, 1ul, 127ul, 1000ul, 1000000ul}) {
+    std::vector<long long> v(n);
+    std::iota(v.begin(), v.end(), 0);
+    const long long ref = std::reduce(v.begin(), v.end(), 10ll);
+    CHECK(std::reduce(pol, v.begin(), v.end(), 10ll) == ref, "stdpar reduce n=%zu", n);
+    CHECK(std::reduce(pol, v.begin(), v.end()) == ref - 10, "stdpar reduce no init n=%zu", n);
+    CHECK(std::reduce(pol, v.begin(), v.end(), 10ll, std::plus<>{}) == ref, "stdpar reduce op n=%zu", n);
+    std::vector<double> a(n), b(n);
+    for (size_t i = 0; i < n; ++i) {
+      a[i] = (double)(i % 11);
+      b[i] = 0.5 * (double)(i % 3);
+    }
+    const double dref = std::transform_reduce(a.begin(), a.end(), b.begin(), 1.0);
+    const double dgot = std::transform_reduce(pol, a.begin(), a.end(), b.begin(), 1.0);
+    CHECK(std::fabs(dgot - dref) <= 1e-9 * std::max(1.0, std::fabs(dref)), "stdpar transform_reduce n=%zu", n);
+  }
+  for (size_t n : {0ul, 1ul, 127ul, 1000ul, 1ul << 20}) {
+    std::vector<int> v(n), out(n), ref(n);
+    std::iota(v.begin(), v.end(), 0);
+    std::inclusive_scan(v.begin(), v.end(), ref.begin());
+    std::inclusive_scan(pol, v.begin(), v.end(), out.begin());
+    CHECK(out == ref, "stdpar inclusive_scan n=%zu", n);
+    std::exclusive_scan(v.begin(), v.end(), ref.begin(), 3);
+    std::exclusive_scan(pol, v.begin(), v.end(), out.begin(), 3);
+    CHECK(out == ref, "stdpar exclusive_scan n=%zu", n);
+    std::vector<unsigned> u(n), uo(n), ur(n);
+    for (size_t i = 0; i < n; ++i) u[i] = 1u + (unsigned)(i % 2);
+    std::inclusive_scan(u.begin(), u.end(), ur.begin(), std::multiplies<unsigned>{}, 3u);
+    std::inclusive_scan(pol, u.begin(), u.end(), uo.begin(), std::multiplies<unsigned>{}, 3u);
+    CHECK(uo == ur, "stdpar inclusive_scan multiplies init 3 n=%zu", n);
+  }
+  for (int mode = 0; mode < 3; ++mode) {
+    std::vector<int> v(1000), out(1000, -1), ref;
+    for (int i = 0; i < 1000; ++i) v[i] = mode == 0 ? 2 * i + 1 : mode == 1 ? 2 * i : i;
+    auto even = [] __host__ __device__(int x) { return x % 2 == 0; };
+    for (int x : v)
+      if (even(x)) ref.push_back(x);
+    auto end = std::copy_if(pol, v.begin(), v.end(), out.begin(), even);
+    CHECK((size_t)(end - out.begin()) == ref.size(), "stdpar copy_if mode %d count", mode);
+    CHECK(std::equal(ref.begin(), ref.end(), out.begin()), "stdpar copy_if mode %d values", mode);
+  }
+  CHECK(!b2p_stdpar::offload_history().empty(), "stdpar offload history recorded");
+}
+
+int main() {
+  try {
+    sycl::queue q;
+    test_algorithms(q);
+    test_reduction(q);
+    test_group_functions(q);
+    test_atomics(q);
+    test_stdpar();
+  } catch (const std::exception &e) {
+    std::printf("FAIL exception: %s\n", e.what());
+    return 2;
+  }
+  if (g_fail) {
+    std::printf("%d of %d checks FAILED\n", g_fail, g_checks);
+    return 1;
+  }
+  std::printf("ALL PASSED %d\n", g_checks);
+  return 0;
+}
