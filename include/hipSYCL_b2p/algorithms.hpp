@@ -206,6 +206,23 @@ constexpr int op_code() {
   else return -1;
 }
 
+// The reference's reductions start every work-item from the operator's
+// identity, and its identity table gives sycl::maximum<T> the value
+// numeric_limits<T>::min() and sycl::minimum<T> numeric_limits<T>::max()
+// (algorithms/numeric.hpp:35-53).  For floating T that is the smallest
+// positive normal / the largest finite value, so a maximum over negative
+// floats returns numeric_limits<T>::min().  Folding that value into init
+// reproduces the reference's results exactly.
+template <class Op, class T>
+T reference_init(T init) {
+  if constexpr (std::is_floating_point_v<T> && std::is_same_v<Op, bs::maximum<T>>)
+    return init < std::numeric_limits<T>::min() ? std::numeric_limits<T>::min() : init;
+  else if constexpr (std::is_floating_point_v<T> && std::is_same_v<Op, bs::minimum<T>>)
+    return std::numeric_limits<T>::max() < init ? std::numeric_limits<T>::max() : init;
+  else
+    return init;
+}
+
 struct identity_fn {
   template <class X>
   B2P_HD X operator()(const X &x) const {
@@ -484,6 +501,7 @@ b2p_sycl::event transform_reduce(b2p_sycl::queue &q, util::allocation_group &scr
   if (first1 == last1) return b2p_sycl::event{};
   q.depends_on(deps);
   const size_t n = (size_t)std::distance(first1, last1);
+  init = detail::reference_init<BinaryReductionOp>(init);
   constexpr int dt = detail::dtype_code<T>();
   if constexpr (detail::is_ptr<ForwardIt1> && detail::is_ptr<ForwardIt2> && (dt == B2P_F32 || dt == B2P_F64) &&
                 std::is_same_v<detail::value_t<ForwardIt1>, T> && std::is_same_v<detail::value_t<ForwardIt2>, T> &&
@@ -513,6 +531,7 @@ b2p_sycl::event transform_reduce(b2p_sycl::queue &q, util::allocation_group &scr
   if (first == last) return b2p_sycl::event{};
   q.depends_on(deps);
   const size_t n = (size_t)std::distance(first, last);
+  init = detail::reference_init<BinaryReductionOp>(init);
   constexpr int dt = detail::dtype_code<T>();
   constexpr int op = detail::op_code<BinaryReductionOp, T>();
   if constexpr (detail::is_ptr<ForwardIt> && dt >= 0 && op >= 0 &&

@@ -167,6 +167,18 @@ static void test_algorithms(sycl::queue &q) {
     auto ev = alg::copy_if(q, g, nothing, nothing, nothing, [] __host__ __device__(int) { return true; }, &cnt);
     CHECK(cnt == 0 && ev.is_complete(), "copy_if empty");
   }
+  // the reference's sycl::maximum<float> identity (numeric_limits<float>::min())
+  {
+    alg::util::allocation_group g{&cache, q.get_device()};
+    float *neg = to_dev(q, std::vector<float>(1000, -2.5f));
+    float *fo = sycl::malloc_shared<float>(1, q);
+    alg::reduce(q, g, neg, neg + 1000, fo, -5.0f, sycl::maximum<float>{}).wait();
+    CHECK(*fo == std::numeric_limits<float>::min(), "reduce maximum<float> identity got %g", *fo);
+    alg::reduce(q, g, neg, neg + 1000, fo, -5.0f, sycl::maximum<>{}).wait();
+    CHECK(*fo == -2.5f, "reduce maximum<> got %g", *fo);
+    sycl::free(neg, q);
+    sycl::free(fo, q);
+  }
   // the cache reuses its allocations
   {
     int *d = to_dev(q, std::vector<int>(5000, 1));
