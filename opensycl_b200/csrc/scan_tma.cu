@@ -1,26 +1,31 @@
-// Pipelined single-pass scan: grid mode 1 of scans whose element and
-// output sizes match (every dtype but bf16).
+// Pipelined single-pass scan and copy_if: grid mode 1 for scans whose
+// element and output sizes match (every dtype but bf16) and for copy_if.
 //
 // Same algorithm as the reference's decoupled look-back scan
 // (algorithms/scan/decoupled_lookback_scan.hpp:555-655: per-tile aggregate,
 // look-back over predecessors' aggregates/prefixes, then the tile's scan
-// from its carry), arranged for B200 as one persistent block per SM with
-// three kinds of warps:
+// from its carry), arranged for B200 as one persistent block per SM in which
+// every step has its own warps, joined by mbarriers on a ring of shared
+// stages:
 //
-//  * a producer warp takes dynamic tile ids in order and streams each tile
-//    into a ring of shared-memory stages with TMA bulk tensor loads
-//    (128-byte swizzle, completion on an mbarrier);
-//  * consumer warps reduce every tile as soon as it lands and publish its
-//    aggregate at once, then emit an older tile (LAG tiles behind) in place
-//    and write it back with a TMA bulk tensor store;
-//  * two look-back warps resolve the carries of the reduced tiles in
-//    parallel (warp-parallel bounded look-back over epoch-tagged 128-bit
-//    status words), so the DRAM latency skew between tiles that the
-//    look-back waits on overlaps with the reduction of later tiles.
+//   producer warp    dynamic tile ids in order; TMA 2-D bulk tensor loads of
+//                    each tile into the next free stage (128-byte swizzle)
+//   reducer warps    as soon as a tile lands: per-thread totals, block scan,
+//                    the thread prefixes kept beside the stage, the tile
+//                    aggregate published at once -- never waiting for carries
+//   look-back warps  two warps resolve the carries of reduced tiles in
+//                    parallel (bounded warp-parallel look-back over
+//                    epoch-tagged 128-bit status words)
+//   emitter warps    as soon as a carry is known: the tile's outputs written
+//                    in place into its stage
+//   store warp       TMA bulk store of each emitted stage, then frees it
 //
-// Elements past the last complete 128-byte row are read and written with
-// plain accesses.  Every wait is bounded; a wait that runs out records
-// B2P_ERR_TIMEOUT in the scratch header and the block leaves its loops.
+// A tile occupies a stage from its load to the end of its store; the
+// reducers run ahead of the emitters by as many tiles as the look-back
+// latency needs, bounded only by the number of stages.  Elements after the
+// last complete 128-byte row use plain loads and stores.  Every wait is
+// bounded; a wait that runs out records B2P_ERR_TIMEOUT in the scratch
+// header and the block leaves its loops.
 #include "scan_tile.cuh"
 #include "tma.cuh"
 #include "internal.h"
@@ -33,9 +38,11 @@ namespace b2p {
 namespace {
 
 constexpr int kMaxStages = 12;
-constexpr int kMaxLag = 6;
 constexpr int kLookWarps = 2;
-constexpr size_t kStageBudget = 196 * 1024;
+constexpr size_t kSmemBudget = 210 * 1024;  // stages + thread prefixes
+
+// Threads of a pipelined block with NC reducer and NC emitter threads.
+constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
 
 struct TmaParams {
   unsigned long long n;
@@ -45,7 +52,8 @@ struct TmaParams {
   int inclusive;
   int has_init;
   unsigned long long init_raw;    // Out-typed init value
-  int stages, lag;
+  int stages;
+  unsigned stage_stride;          // bytes between stages
   const void *in;
   void *out;
   ScratchHeader *hdr;
@@ -58,29 +66,45 @@ struct TmaParams {
   unsigned long long *num_copied;
 };
 
-// Block-shared state of the pipeline: per stage, the TMA fill barrier
-// (full), the stage-free barrier (empty), the aggregate-published barrier
-// (aggr: consumers -> look-back warps) and the carry-ready barrier (cready:
-// look-back warps -> consumers), with the stage's tile id, aggregate and
-// carry.
+// Block-shared state of the pipeline.  Per stage: the TMA fill barrier
+// (full: producer -> reducers), aggregate published (aggr: reducers ->
+// look-back warps), carry known (cready: look-back warps -> emitters),
+// outputs in place (emitted: emitters -> store warp), stage free (empty:
+// store warp -> producer); the stage's tile id, aggregate and carry.
 struct PipeState {
-  uint64_t full[kMaxStages], empty[kMaxStages], aggr[kMaxStages], cready[kMaxStages];
+  uint64_t full[kMaxStages], empty[kMaxStages], aggr[kMaxStages], cready[kMaxStages], emitted[kMaxStages];
   long long tile[kMaxStages];
   unsigned long long agg[kMaxStages], carry[kMaxStages];
   unsigned long long epoch;
-  long long end_item;
+  long long end_item;  // number of tiles this block handles, once the reducers know it
 };
 
-// Thread total over ITEMS consecutive elements of a full tile.
+// Position in the ring of stages: stage index and mbarrier phase parity of
+// an item, advanced without divisions.
+struct RingPos {
+  int s = 0;
+  unsigned ph = 0;
+  __device__ __forceinline__ void advance(int k, int S) {
+    s += k;
+    while (s >= S) {
+      s -= S;
+      ph ^= 1u;
+    }
+  }
+};
+
+// --------------------------------------------------- per-thread tile passes
+// `t` is the thread's index inside its warp group (reducers or emitters).
+
 template <class P, int ITEMS>
-__device__ __forceinline__ typename P::Acc thread_total_full(const char *buf) {
+__device__ __forceinline__ typename P::Acc thread_total_t(const char *buf, int t) {
   using In = typename P::In;
   constexpr int IPV = 16 / (int)sizeof(In);
   constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
   typename P::Acc agg = P::identity();
 #pragma unroll
   for (int k = 0; k < VPT; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
     const In *e = reinterpret_cast<const In *>(&w);
 #pragma unroll
     for (int q = 0; q < IPV; ++q) P::add(agg, e[q]);
@@ -89,16 +113,16 @@ __device__ __forceinline__ typename P::Acc thread_total_full(const char *buf) {
   return agg;
 }
 
-// fp32 SUM, pass 1: compensated (TwoSum) running sums of the thread's
-// elements from zero, written back in place rounded to fp32 (inclusive: after
-// adding the element, exclusive: before).  Returns the thread total.
+// fp32 SUM, reducer pass: compensated (TwoSum) running sums of the thread's
+// elements from zero, written back in place rounded to fp32 (inclusive:
+// after adding the element, exclusive: before).  Returns the thread total.
 template <int ITEMS, bool INCLUSIVE>
-__device__ __forceinline__ DF thread_runs_f32(char *buf) {
+__device__ __forceinline__ DF thread_runs_f32(char *buf, int t) {
   constexpr int VPT = ITEMS / 4;
   DF run{0.f, 0.f};
 #pragma unroll
   for (int k = 0; k < VPT; ++k) {
-    float4 *slot = reinterpret_cast<float4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    float4 *slot = reinterpret_cast<float4 *>(buf + swz(t * VPT + k) * 16);
     float4 w = *slot;
     float *e = reinterpret_cast<float *>(&w);
 #pragma unroll
@@ -117,15 +141,15 @@ __device__ __forceinline__ DF thread_runs_f32(char *buf) {
   return df_norm(run);
 }
 
-// fp32 SUM, pass 2: output = start + run.  The run carries at most one
+// fp32 SUM, emitter pass: output = start + run.  The run carries at most one
 // rounding of its exact value, so each output is within ~2 ulp of the exact
 // prefix for same-signed data.
 template <int ITEMS>
-__device__ __forceinline__ void emit_f32_runs(char *buf, DF start) {
+__device__ __forceinline__ void emit_f32_runs(char *buf, DF start, int t) {
   constexpr int VPT = ITEMS / 4;
 #pragma unroll
   for (int k = 0; k < VPT; ++k) {
-    float4 *slot = reinterpret_cast<float4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
+    float4 *slot = reinterpret_cast<float4 *>(buf + swz(t * VPT + k) * 16);
     float4 w = *slot;
     w.x = __fadd_rn(start.hi, __fadd_rn(start.lo, w.x));
     w.y = __fadd_rn(start.hi, __fadd_rn(start.lo, w.y));
@@ -135,15 +159,43 @@ __device__ __forceinline__ void emit_f32_runs(char *buf, DF start) {
   }
 }
 
-// Block exclusive scan over the NC consumer threads (named barrier 1; the
-// producer and look-back warps do not take part).
+// Generic emitter pass: the thread's outputs from its running value, in place.
+template <class P, int ITEMS>
+__device__ __forceinline__ void emit_generic(char *buf, typename P::Acc run, bool inclusive, int t) {
+  using In = typename P::In;
+  using Out = typename P::Out;
+  static_assert(sizeof(In) == sizeof(Out), "in place");
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    uint4 *slot = reinterpret_cast<uint4 *>(buf + swz(t * VPT + k) * 16);
+    const uint4 w = *slot;
+    const In *e = reinterpret_cast<const In *>(&w);
+    uint4 o;
+    Out *oe = reinterpret_cast<Out *>(&o);
+#pragma unroll
+    for (int q = 0; q < IPV; ++q) {
+      if (inclusive) {
+        P::add(run, e[q]);
+        oe[q] = P::finalize(run);
+      } else {
+        oe[q] = P::finalize(run);
+        P::add(run, e[q]);
+      }
+    }
+    *slot = o;
+  }
+}
+
+// Exclusive scan over one warp group of NC threads (named barrier `bar`);
+// t = index in the group.
 template <class Ops, int NC>
-__device__ __forceinline__ typename Ops::Pub consumer_exclusive_scan(typename Ops::Pub v,
-                                                                     typename Ops::Pub *s_warp,
-                                                                     typename Ops::Pub *total) {
+__device__ __forceinline__ typename Ops::Pub group_exclusive_scan(typename Ops::Pub v, typename Ops::Pub *s_warp,
+                                                                  typename Ops::Pub *total, int t, int bar) {
   using Pub = typename Ops::Pub;
   constexpr int kWarps = NC / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = t & 31, warp = t >> 5;
   Pub incl = v;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -151,7 +203,7 @@ __device__ __forceinline__ typename Ops::Pub consumer_exclusive_scan(typename Op
     if (lane >= d) incl = Ops::combine(o, incl);
   }
   if (lane == 31) s_warp[warp] = incl;
-  bar_named(1, NC);
+  bar_named(bar, NC);
   if (warp == 0) {
     Pub w = lane < kWarps ? s_warp[lane] : Ops::identity();
 #pragma unroll
@@ -161,27 +213,13 @@ __device__ __forceinline__ typename Ops::Pub consumer_exclusive_scan(typename Op
     }
     if (lane < kWarps) s_warp[lane] = w;
   }
-  bar_named(1, NC);
+  bar_named(bar, NC);
   Pub ex = shfl_up(incl, 1);
   if (lane == 0) ex = Ops::identity();
   if (warp > 0) ex = Ops::combine(s_warp[warp - 1], ex);
   *total = s_warp[kWarps - 1];
-  return ex;
+  return ex;  // callers end with a bar_named(bar, NC) before s_warp is used again
 }
-
-// Position in the ring of S stages: stage index and mbarrier phase parity
-// of an item, advanced without divisions.
-struct RingPos {
-  int s = 0;
-  unsigned ph = 0;
-  __device__ __forceinline__ void advance(int k, int S) {
-    s += k;
-    while (s >= S) {
-      s -= S;
-      ph ^= 1u;
-    }
-  }
-};
 
 // Carry of tile 0 (init, or the identity), in the published representation.
 template <class P, bool WIDE>
@@ -196,6 +234,8 @@ __device__ __forceinline__ unsigned long long tile0_carry(const TmaParams &p) {
   else return P::pack(P::from_out(v));
 }
 
+// ------------------------------------------------------------ warp roles
+
 // Thread 0 of the block: barriers and the launch epoch.
 __device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
   if (threadIdx.x == 0) {
@@ -204,6 +244,7 @@ __device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
       mbar_init(&ps.empty[i], 1);
       mbar_init(&ps.aggr[i], 1);
       mbar_init(&ps.cready[i], 1);
+      mbar_init(&ps.emitted[i], 1);
     }
     mbar_init_fence();
     ps.epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
@@ -211,12 +252,11 @@ __device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
   }
 }
 
-// Producer (one thread): dynamic tile ids in order; each tile's complete
-// rows streamed into the next free stage (stages `stride` bytes apart) in
-// boxes of `box` rows.  A tile past the last complete row completes its
-// stage without a copy.  Tile id -1 ends the consumers.
+// Producer (one thread): each tile's complete rows into the next free stage
+// in boxes of `box` rows.  A tile wholly past the complete rows completes
+// its stage without a copy.  Tile id -1 ends the reducers.
 __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaParams &p, PipeState &ps,
-                                              char *smem, unsigned stride, int rows, int box) {
+                                              char *smem, int rows, int box) {
   prefetch_tensormap(tin);
   const unsigned long long pol = l2_policy_stream();
   const int S = p.stages;
@@ -243,15 +283,15 @@ __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaP
     } else {
       mbar_arrive_expect_tx(&ps.full[s], (unsigned)nbox * (unsigned)box * 128u);
       for (int b = 0; b < nbox; ++b)
-        tma_load_2d(smem + (size_t)s * stride + (size_t)b * box * 128, tin, 0, (int)(r0 + (long long)b * box),
-                    &ps.full[s], pol);
+        tma_load_2d(smem + (size_t)s * p.stage_stride + (size_t)b * box * 128, tin, 0,
+                    (int)(r0 + (long long)b * box), &ps.full[s], pol);
     }
   }
 }
 
 // Look-back warp wi of kLookWarps: items wi, wi + kLookWarps, ... in stage
 // order.  Resolves each reduced tile's carry, publishes its inclusive prefix
-// and hands the carry to the consumers.
+// and hands the carry to the emitters.
 template <class Ops>
 __device__ __forceinline__ void lookback_loop(const TmaParams &p, PipeState &ps, int wi,
                                               unsigned long long init_bits, unsigned long long epoch_tag) {
@@ -290,17 +330,33 @@ __device__ __forceinline__ void lookback_loop(const TmaParams &p, PipeState &ps,
   }
 }
 
-// Consumer thread 0 after the last item: end the look-back warps (they wait
-// on items it .. it + kLookWarps - 1) and the outstanding bulk stores.
-__device__ __forceinline__ void consumers_finish(const TmaParams &p, PipeState &ps, long long it, RingPos rr) {
-  if (threadIdx.x == 0) {
-    bulk_wait_all();
-    ps.end_item = it;
-    for (int j = 0; j < kLookWarps; ++j, rr.advance(1, p.stages)) mbar_arrive(&ps.aggr[rr.s]);
+// Emitter group: wait for item `it`'s carry, or learn that the block's items
+// are exhausted (the reducers publish the count when they meet the end).
+// Returns 1 = carry ready, 0 = no more items, -1 = timeout.
+__device__ __forceinline__ int emitter_wait(const TmaParams &p, PipeState &ps, const RingPos &r, long long it) {
+  uint64_t t0 = 0;
+  for (unsigned k = 0;; ++k) {
+    if (mbar_try(&ps.cready[r.s], r.ph)) return 1;
+    if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) return 0;
+    if ((k & 31) == 31) {
+      const uint64_t now = globaltimer_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > p.timeout_ns) return -1;
+    }
   }
 }
 
-// Elements past the complete rows (only in the last tile) into the stage.
+// Emitter leader after the last item (`it` = item count): every earlier item
+// passed the look-back warps and was handed to the store warp, so their
+// barriers are in step; end the look-back warps (waiting on items it and
+// it + 1) and the store warp (waiting on item it).
+__device__ __forceinline__ void emitters_finish(const TmaParams &p, PipeState &ps, RingPos r) {
+  mbar_arrive(&ps.emitted[r.s]);
+  for (int j = 0; j < kLookWarps; ++j, r.advance(1, p.stages)) mbar_arrive(&ps.aggr[r.s]);
+}
+
+// Elements past the complete rows (only in the last tile) into the stage,
+// by the reducer group (threads 0 .. ntail-1 of the block).
 template <class T, int NC>
 __device__ __forceinline__ void load_row_tail(const TmaParams &p, char *buf, long long tile, int tile_elems) {
   const int ntail = (int)(p.n - p.tail_begin);
@@ -311,8 +367,10 @@ __device__ __forceinline__ void load_row_tail(const TmaParams &p, char *buf, lon
   bar_named(1, NC);
 }
 
+// ------------------------------------------------------------------- scan
+
 template <class P, int NC, int ITEMS, bool WIDE>
-__global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
+__global__ void __launch_bounds__(pipe_threads(NC), 1)
     scan_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
                     TmaParams p) {
   using In = typename P::In;
@@ -326,11 +384,12 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
   constexpr int kRows = kTile / kEpr;
   constexpr int kBox = kRows < 256 ? kRows : 256;
   static_assert(kRows % kBox == 0, "box rows");
-  constexpr unsigned kStageBytes = (unsigned)kRows * 128u;
   constexpr bool kFast = std::is_same<P, FloatSumPolicy<float>>::value;
 
   extern __shared__ char smem_raw[];
   char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // thread prefixes of every stage, after the stages
+  Acc *texcl_all = reinterpret_cast<Acc *>(smem + (size_t)p.stages * p.stage_stride);
   __shared__ __align__(8) PipeState ps;
   __shared__ Acc s_warp[32];
 
@@ -340,85 +399,32 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
   const unsigned long long epoch_tag = epoch << 8;
   const unsigned long long init_bits = tile0_carry<P, WIDE>(p);
   const int warp = threadIdx.x >> 5;
+  const int S = p.stages;
+  const long long last = p.ntiles - 1;
+  const int ntail = (int)(p.n - p.tail_begin);
 
-  if (warp == NC / 32 + kLookWarps) {
-    if ((threadIdx.x & 31) == 0) {
-      prefetch_tensormap(&tout);
-      producer_loop(&tin, p, ps, smem, kStageBytes, kRows, kBox);
-    }
-  } else if (warp >= NC / 32) {
-    lookback_loop<Ops>(p, ps, warp - NC / 32, init_bits, epoch_tag);
-  } else {
-    const unsigned long long spol = l2_policy_stream();
-    const int S = p.stages, LAG = p.lag;
-    const long long last = p.ntiles - 1;
-    const int ntail = (int)(p.n - p.tail_begin);
-    Out *out = reinterpret_cast<Out *>(p.out);
-    Acc q[kMaxLag + 1];  // thread prefixes of reduced, not yet emitted tiles (oldest first)
-#pragma unroll
-    for (int i = 0; i <= kMaxLag; ++i) q[i] = P::identity();
-    int npend = 0;
+  if (warp < NC / 32) {
+    // ------------------------------------------------------------ reducers
+    const int t = threadIdx.x;
     long long it = 0;
-    bool ok = true;
-    RingPos er, rr;   // ring positions of the next item to emit / to reduce
-    int prev_s = -1;  // stage of the previous emission (its store may still read it)
-
-    auto emit_one = [&]() -> bool {
-      const int s = er.s;
-      if (!mbar_wait(&ps.cready[s], er.ph, p.timeout_ns)) {
-        if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        return false;
-      }
-      const long long tile = ps.tile[s];
-      char *buf = smem + (size_t)s * kStageBytes;
-      const Acc texcl = q[0];
-#pragma unroll
-      for (int i = 0; i < kMaxLag; ++i) q[i] = q[i + 1];
-      const Acc start = start_value<P, WIDE>(ps.carry[s], texcl);
-      if constexpr (kFast) emit_f32_runs<ITEMS>(buf, start);
-      else emit_scan<P, ITEMS>(buf, buf, start, p.inclusive != 0);
-      fence_async_smem();
-      bar_named(1, NC);
-      if (tile == last && ntail > 0) {
-        const long long j0 = (long long)p.tail_begin - tile * kTile;
-        if ((int)threadIdx.x < ntail)
-          out[p.tail_begin + threadIdx.x] = *smem_elem_ptr<Out>(buf, (int)j0 + (int)threadIdx.x);
-        bar_named(1, NC);
-      }
-      if (threadIdx.x == 0) {
-        const long long r0 = tile * kRows;
-        const long long rows_out = min((long long)kRows, p.rows_full - r0);
-        for (long long r = 0; r < rows_out; r += kBox)
-          tma_store_2d(&tout, 0, (int)(r0 + r), buf + r * 128, spol);
-        bulk_commit();
-        bulk_wait_read<1>();  // the previous emission's store has read its stage
-        if (prev_s >= 0) mbar_arrive(&ps.empty[prev_s]);
-      }
-      prev_s = s;
-      er.advance(1, S);
-      return true;
-    };
-
-    for (;; ++it, rr.advance(1, S)) {
-      const int s = rr.s;
-      if (!mbar_wait(&ps.full[s], rr.ph, p.timeout_ns)) {
-        if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        ok = false;
+    RingPos r;
+    for (;; ++it, r.advance(1, S)) {
+      const int s = r.s;
+      if (!mbar_wait(&ps.full[s], r.ph, p.timeout_ns)) {
+        if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         break;
       }
       const long long tile = ps.tile[s];
       if (tile < 0) break;
-      char *buf = smem + (size_t)s * kStageBytes;
+      char *buf = smem + (size_t)s * p.stage_stride;
       if (tile == last && ntail > 0) load_row_tail<In, NC>(p, buf, tile, kTile);
       Acc agg;
-      if constexpr (kFast) agg = p.inclusive ? thread_runs_f32<ITEMS, true>(buf) : thread_runs_f32<ITEMS, false>(buf);
-      else agg = thread_total_full<P, ITEMS>(buf);
+      if constexpr (kFast) agg = p.inclusive ? thread_runs_f32<ITEMS, true>(buf, t) : thread_runs_f32<ITEMS, false>(buf, t);
+      else agg = thread_total_t<P, ITEMS>(buf, t);
       Acc tile_agg;
-      const Acc texcl = consumer_exclusive_scan<AccOps<P>, NC>(agg, s_warp, &tile_agg);
-#pragma unroll
-      for (int i = 0; i <= kMaxLag; ++i)
-        if (i == npend) q[i] = texcl;
-      if (threadIdx.x == 0) {
+      texcl_all[(size_t)s * NC + t] = group_exclusive_scan<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
+      bar_named(1, NC);  // every thread prefix (and fp32 run) is in place
+      if (t == 0) {
         const unsigned long long bits = publish_value<P, WIDE>(tile_agg);
         if (tile != p.stall_tile) {
           if (tile == 0)
@@ -428,37 +434,80 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
             st_status(p.status + tile, bits, epoch_tag | kFlagAgg);
         }
         ps.agg[s] = bits;
-        mbar_arrive(&ps.aggr[s]);
+        mbar_arrive(&ps.aggr[s]);  // releases the thread prefixes and the in-place runs too
       }
-      ++npend;
-      if (npend > LAG) {
-        if (!emit_one()) {
-          ok = false;
+    }
+    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
+  } else if (warp < 2 * NC / 32) {
+    // ------------------------------------------------------------ emitters
+    const int t = threadIdx.x - NC;
+    Out *out = reinterpret_cast<Out *>(p.out);
+    RingPos r;
+    for (long long it = 0;; ++it, r.advance(1, S)) {
+      const int w = emitter_wait(p, ps, r, it);
+      if (w <= 0) {
+        if (w < 0 && t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        if (w == 0 && t == 0) emitters_finish(p, ps, r);
+        break;
+      }
+      const int s = r.s;
+      const long long tile = ps.tile[s];
+      char *buf = smem + (size_t)s * p.stage_stride;
+      const Acc start = start_value<P, WIDE>(ps.carry[s], texcl_all[(size_t)s * NC + t]);
+      if constexpr (kFast) emit_f32_runs<ITEMS>(buf, start, t);
+      else emit_generic<P, ITEMS>(buf, start, p.inclusive != 0, t);
+      fence_async_smem();
+      bar_named(2, NC);
+      if (tile == last && ntail > 0) {
+        const long long j0 = (long long)p.tail_begin - tile * kTile;
+        if (t < ntail) out[p.tail_begin + t] = *smem_elem_ptr<Out>(buf, (int)j0 + t);
+        bar_named(2, NC);
+      }
+      if (t == 0) mbar_arrive(&ps.emitted[s]);
+    }
+  } else if (warp < 2 * NC / 32 + kLookWarps) {
+    lookback_loop<Ops>(p, ps, warp - 2 * NC / 32, init_bits, epoch_tag);
+  } else if (warp == 2 * NC / 32 + kLookWarps) {
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox);
+  } else {
+    // ---------------------------------------------------------- store warp
+    if ((threadIdx.x & 31) == 0) {
+      prefetch_tensormap(&tout);
+      const unsigned long long spol = l2_policy_stream();
+      RingPos r;
+      for (long long it = 0;; ++it, r.advance(1, S)) {
+        const int s = r.s;
+        if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
+          record_error(p.hdr, B2P_ERR_TIMEOUT);
           break;
         }
-        --npend;
+        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+        const long long tile = ps.tile[s];
+        const long long r0 = tile * kRows;
+        const long long rows_out = min((long long)kRows, p.rows_full - r0);
+        for (long long rr = 0; rr < rows_out; rr += kBox)
+          tma_store_2d(&tout, 0, (int)(r0 + rr), smem + (size_t)s * p.stage_stride + rr * 128, spol);
+        bulk_commit();
+        bulk_wait_read<0>();
+        mbar_arrive(&ps.empty[s]);
       }
+      bulk_wait_all();
     }
-    if (ok) {
-      while (npend > 0) {
-        if (!emit_one()) break;
-        --npend;
-      }
-    }
-    consumers_finish(p, ps, it, rr);
   }
   finish_launch(p.hdr, epoch, nullptr, 0);
 }
 
-// Order-preserving compaction (copy_if) on the same pipeline.  A tile's
-// aggregate is its kept count; its carry is the output position of its
-// first kept element.  At emission the kept elements are packed, in order,
-// into the stage with the output's 16-byte phase, the 16-byte-aligned middle
-// is written with one bulk copy and the unaligned ends with plain stores.
-// Stages are kStageBytes + 1024 apart: packing may shift the tile by up to
-// 15 bytes.
+// ---------------------------------------------------------------- copy_if
+
+// Order-preserving compaction on the same pipeline.  A tile's aggregate is
+// its kept count; its carry is the output position of its first kept
+// element.  The emitters pack the kept elements, in order, into the stage
+// with the output's 16-byte phase and write the unaligned ends with plain
+// stores; the store warp writes the 16-byte-aligned middle with one bulk
+// copy.  Stages are 1024 bytes longer than a tile: packing may shift it by
+// up to 15 bytes.
 template <class T, int NC, int ITEMS>
-__global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
+__global__ void __launch_bounds__(pipe_threads(NC), 1)
     copy_if_tma_kernel(const __grid_constant__ CUtensorMap tin, TmaParams p) {
   constexpr int kTile = NC * ITEMS;
   constexpr int kEpr = 128 / (int)sizeof(T);
@@ -466,13 +515,13 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
   constexpr int kRows = kTile / kEpr;
   constexpr int kBox = kRows < 256 ? kRows : 256;
   static_assert(kRows % kBox == 0, "box rows");
-  constexpr unsigned kStride = (unsigned)kRows * 128u + 1024u;
   constexpr int EPV = 16 / (int)sizeof(T);
   constexpr int VPT = ITEMS / EPV;
   static_assert(ITEMS <= 32, "keep mask is 32 bits");
 
   extern __shared__ char smem_raw[];
   char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned long long *texcl_all = reinterpret_cast<unsigned long long *>(smem + (size_t)p.stages * p.stage_stride);
   __shared__ __align__(8) PipeState ps;
   __shared__ unsigned long long s_warp[32];
 
@@ -481,76 +530,92 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
   const unsigned long long epoch = ps.epoch;
   const unsigned long long epoch_tag = epoch << 8;
   const int warp = threadIdx.x >> 5;
+  const int S = p.stages;
+  const long long last = p.ntiles - 1;
+  const int ntail = (int)(p.n - p.tail_begin);
+  T *out = reinterpret_cast<T *>(p.out);
 
-  if (warp == NC / 32 + kLookWarps) {
-    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kStride, kRows, kBox);
-  } else if (warp >= NC / 32) {
-    lookback_loop<CountOps>(p, ps, warp - NC / 32, 0ull, epoch_tag);
-  } else {
-    const int S = p.stages, LAG = p.lag;
-    const long long last = p.ntiles - 1;
-    const int ntail = (int)(p.n - p.tail_begin);
-    T *out = reinterpret_cast<T *>(p.out);
-    unsigned long long q[kMaxLag + 1];
+  // predicate flags of thread t's elements of a tile (the first `count`
+  // elements of the tile are real)
+  auto flags = [&](const char *buf, int t, int count, uint4 (&v)[VPT], int *kept) -> unsigned {
+    const int first = t * ITEMS;
+    unsigned keep = 0;
+    int c = 0;
 #pragma unroll
-    for (int i = 0; i <= kMaxLag; ++i) q[i] = 0;
-    int npend = 0;
-    long long it = 0;
-    bool ok = true;
-    RingPos er, rr;
-    int prev_s = -1;
-
-    // predicate flags of this thread's elements of a tile (count valid ones)
-    auto flags = [&](const uint4 (&v)[VPT], int count, int *kept) -> unsigned {
-      const int first = threadIdx.x * ITEMS;
-      unsigned keep = 0;
-      int c = 0;
+    for (int k = 0; k < VPT; ++k) {
+      v[k] = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+      const T *e = reinterpret_cast<const T *>(&v[k]);
 #pragma unroll
-      for (int k = 0; k < VPT; ++k) {
-        const T *e = reinterpret_cast<const T *>(&v[k]);
-#pragma unroll
-        for (int qq = 0; qq < EPV; ++qq) {
-          const int j = k * EPV + qq;
-          const bool kb = (first + j < count) && pred_bits(e[qq], p.mask, p.cmp, p.rhs);
-          keep |= (unsigned)kb << j;
-          c += kb;
-        }
+      for (int qq = 0; qq < EPV; ++qq) {
+        const int j = k * EPV + qq;
+        const bool kb = (first + j < count) && pred_bits(e[qq], p.mask, p.cmp, p.rhs);
+        keep |= (unsigned)kb << j;
+        c += kb;
       }
-      *kept = c;
-      return keep;
-    };
-    auto load_v = [&](const char *buf, uint4 (&v)[VPT]) {
-#pragma unroll
-      for (int k = 0; k < VPT; ++k) v[k] = *reinterpret_cast<const uint4 *>(buf + swz(threadIdx.x * VPT + k) * 16);
-    };
+    }
+    *kept = c;
+    return keep;
+  };
 
-    auto emit_one = [&]() -> bool {
-      const int s = er.s;
-      if (!mbar_wait(&ps.cready[s], er.ph, p.timeout_ns)) {
-        if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        return false;
+  if (warp < NC / 32) {
+    // ------------------------------------------------------------ reducers
+    const int t = threadIdx.x;
+    long long it = 0;
+    RingPos r;
+    for (;; ++it, r.advance(1, S)) {
+      const int s = r.s;
+      if (!mbar_wait(&ps.full[s], r.ph, p.timeout_ns)) {
+        if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        break;
       }
       const long long tile = ps.tile[s];
-      char *buf = smem + (size_t)s * kStride;
-      const unsigned long long texcl = q[0];
-#pragma unroll
-      for (int i = 0; i < kMaxLag; ++i) q[i] = q[i + 1];
+      if (tile < 0) break;
+      char *buf = smem + (size_t)s * p.stage_stride;
+      if (tile == last && ntail > 0) load_row_tail<T, NC>(p, buf, tile, kTile);
+      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
+      uint4 v[VPT];
+      int kept;
+      (void)flags(buf, t, count, v, &kept);
+      unsigned long long tile_kept;
+      texcl_all[(size_t)s * NC + t] =
+          group_exclusive_scan<CountOps, NC>((unsigned long long)kept, s_warp, &tile_kept, t, 1);
+      bar_named(1, NC);  // every thread prefix is in place
+      if (t == 0) {
+        if (tile != p.stall_tile)
+          st_status(p.status + tile, tile_kept, epoch_tag | (tile == 0 ? kFlagPrefix : kFlagAgg));
+        ps.agg[s] = tile_kept;
+        mbar_arrive(&ps.aggr[s]);
+      }
+    }
+    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
+  } else if (warp < 2 * NC / 32) {
+    // ------------------------------------------------------------ emitters
+    const int t = threadIdx.x - NC;
+    RingPos r;
+    for (long long it = 0;; ++it, r.advance(1, S)) {
+      const int w = emitter_wait(p, ps, r, it);
+      if (w <= 0) {
+        if (w < 0 && t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        if (w == 0 && t == 0) emitters_finish(p, ps, r);
+        break;
+      }
+      const int s = r.s;
+      const long long tile = ps.tile[s];
+      char *buf = smem + (size_t)s * p.stage_stride;
       const unsigned long long carry = ps.carry[s];
       unsigned long long kept_total = ps.agg[s];
       if (carry > p.n || kept_total > p.n - carry) {  // only after a broken chain: write nothing
-        if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         kept_total = 0;
       }
       const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
       uint4 v[VPT];
-      load_v(buf, v);
       int kept;
-      const unsigned keep = flags(v, count, &kept);
-      bar_named(1, NC);  // every thread holds its elements: the stage may be overwritten
-      // pack with the output's 16-byte phase: element k at byte phase + k * sizeof(T)
+      const unsigned keep = flags(buf, t, count, v, &kept);
+      bar_named(2, NC);  // every emitter holds its elements: the stage may be overwritten
       const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
       const unsigned phase = (unsigned)(g0 & 15u);
-      unsigned long long o = texcl;
+      unsigned long long o = texcl_all[(size_t)s * NC + t];
 #pragma unroll
       for (int k = 0; k < VPT; ++k) {
         const T *e = reinterpret_cast<const T *>(&v[k]);
@@ -562,83 +627,55 @@ __global__ void __launch_bounds__(NC + 32 * kLookWarps + 32, 1)
           }
       }
       fence_async_smem();
-      bar_named(1, NC);
+      bar_named(2, NC);
       const uintptr_t g1 = g0 + kept_total * sizeof(T);
       const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
       const bool mid = a1 > a0;
       const long long nhead = mid ? (long long)((a0 - g0) / sizeof(T)) : (long long)kept_total;
       const long long tail0 = mid ? (long long)((a1 - g0) / sizeof(T)) : (long long)kept_total;
       const long long ntl = (long long)kept_total - tail0;
-      if ((long long)threadIdx.x < nhead)
-        out[carry + threadIdx.x] = *reinterpret_cast<const T *>(buf + phase + threadIdx.x * sizeof(T));
-      if (threadIdx.x >= 32 && (long long)threadIdx.x - 32 < ntl) {
-        const long long k = tail0 + (threadIdx.x - 32);
+      if (t < nhead) out[carry + t] = *reinterpret_cast<const T *>(buf + phase + t * sizeof(T));
+      if (t >= 32 && t - 32 < ntl) {
+        const long long k = tail0 + (t - 32);
         out[carry + k] = *reinterpret_cast<const T *>(buf + phase + k * sizeof(T));
       }
-      if (threadIdx.x == 0) {
-        if (mid) {
-          const unsigned bytes = (unsigned)(a1 - a0);
+      if (t == 0 && tile == last && p.num_copied) *p.num_copied = carry + kept_total;
+      bar_named(2, NC);  // the plain stores are done with the stage
+      if (t == 0) mbar_arrive(&ps.emitted[s]);
+    }
+  } else if (warp < 2 * NC / 32 + kLookWarps) {
+    lookback_loop<CountOps>(p, ps, warp - 2 * NC / 32, 0ull, epoch_tag);
+  } else if (warp == 2 * NC / 32 + kLookWarps) {
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox);
+  } else {
+    // ---------------------------------------------------------- store warp
+    if ((threadIdx.x & 31) == 0) {
+      RingPos r;
+      for (long long it = 0;; ++it, r.advance(1, S)) {
+        const int s = r.s;
+        if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
+          record_error(p.hdr, B2P_ERR_TIMEOUT);
+          break;
+        }
+        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+        const unsigned long long carry = ps.carry[s];
+        unsigned long long kept_total = ps.agg[s];
+        if (carry > p.n || kept_total > p.n - carry) kept_total = 0;
+        const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
+        const uintptr_t g1 = g0 + kept_total * sizeof(T);
+        const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
+        if (a1 > a0) {
+          const char *src = smem + (size_t)s * p.stage_stride + (g0 & 15u) + (a0 - g0);
           asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(a0),
-                       "r"(smem_u32(buf + phase + (a0 - g0))), "r"(bytes)
+                       "r"(smem_u32(src)), "r"((unsigned)(a1 - a0))
                        : "memory");
         }
         bulk_commit();
-        if (tile == last && p.num_copied) *p.num_copied = carry + kept_total;
+        bulk_wait_read<0>();
+        mbar_arrive(&ps.empty[s]);
       }
-      bar_named(1, NC);  // plain stores of the ends done before the stage can be released
-      if (threadIdx.x == 0) {
-        bulk_wait_read<1>();
-        if (prev_s >= 0) mbar_arrive(&ps.empty[prev_s]);
-      }
-      prev_s = s;
-      er.advance(1, S);
-      return true;
-    };
-
-    for (;; ++it, rr.advance(1, S)) {
-      const int s = rr.s;
-      if (!mbar_wait(&ps.full[s], rr.ph, p.timeout_ns)) {
-        if (threadIdx.x == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        ok = false;
-        break;
-      }
-      const long long tile = ps.tile[s];
-      if (tile < 0) break;
-      char *buf = smem + (size_t)s * kStride;
-      if (tile == last && ntail > 0) load_row_tail<T, NC>(p, buf, tile, kTile);
-      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
-      uint4 v[VPT];
-      load_v(buf, v);
-      int kept;
-      (void)flags(v, count, &kept);
-      unsigned long long tile_kept;
-      const unsigned long long texcl =
-          consumer_exclusive_scan<CountOps, NC>((unsigned long long)kept, s_warp, &tile_kept);
-#pragma unroll
-      for (int i = 0; i <= kMaxLag; ++i)
-        if (i == npend) q[i] = texcl;
-      if (threadIdx.x == 0) {
-        if (tile != p.stall_tile)
-          st_status(p.status + tile, tile_kept, epoch_tag | (tile == 0 ? kFlagPrefix : kFlagAgg));
-        ps.agg[s] = tile_kept;
-        mbar_arrive(&ps.aggr[s]);
-      }
-      ++npend;
-      if (npend > LAG) {
-        if (!emit_one()) {
-          ok = false;
-          break;
-        }
-        --npend;
-      }
+      bulk_wait_all();
     }
-    if (ok) {
-      while (npend > 0) {
-        if (!emit_one()) break;
-        --npend;
-      }
-    }
-    consumers_finish(p, ps, it, rr);
   }
   finish_launch(p.hdr, epoch, nullptr, 0);
 }
@@ -667,10 +704,10 @@ EncodeTiledFn encode_fn() {
 template <class P, int NC, int ITEMS, bool WIDE>
 int launch_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, cudaStream_t st) {
   auto kfn = scan_tma_kernel<P, NC, ITEMS, WIDE>;
-  const size_t smem = (size_t)p.stages * NC * ITEMS * sizeof(typename P::In) + 1024;
+  const size_t smem = (size_t)p.stages * (p.stage_stride + NC * sizeof(typename P::Acc)) + 1024;
   int rc = ensure_dynamic_smem((const void *)kfn, smem);
   if (rc) return rc;
-  const int threads = NC + 32 * kLookWarps + 32;
+  const int threads = pipe_threads(NC);
   if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
   const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
   kfn<<<grid, threads, smem, st>>>(tin, tout, p);
@@ -683,7 +720,6 @@ int launch_policy(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout,
   if (block == 128 && items == 32) return launch_shape<P, 128, 32, WIDE>(p, tin, tout, st);
   if (block == 256 && items == 16) return launch_shape<P, 256, 16, WIDE>(p, tin, tout, st);
   if (block == 256 && items == 32) return launch_shape<P, 256, 32, WIDE>(p, tin, tout, st);
-  if (block == 512 && items == 16) return launch_shape<P, 512, 16, WIDE>(p, tin, tout, st);
   return B2P_ERR_UNSUPPORTED;
 }
 
@@ -695,7 +731,7 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
   const size_t es = sizeof(In);
   const long long tile = (long long)block * items;
   const size_t stage = (size_t)tile * es;
-  const int stages = (int)std::min<size_t>(kMaxStages, kStageBudget / stage);
+  const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stage + block * sizeof(typename P::Acc)));
   if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
@@ -706,7 +742,7 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
   if (p.rows_full + tile / epr >= (1ll << 31)) return B2P_ERR_UNSUPPORTED;
   p.inclusive = inclusive;
   p.stages = stages;
-  p.lag = std::max(1, std::min(kMaxLag, stages - 3));
+  p.stage_stride = (unsigned)stage;
   p.in = in;
   p.out = out;
   p.hdr = reinterpret_cast<ScratchHeader *>(scratch);
@@ -756,10 +792,10 @@ int dispatch(int op, int inclusive, const void *in, void *out, size_t n, const v
 template <class T, int NC, int ITEMS>
 int launch_copy_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
   auto kfn = copy_if_tma_kernel<T, NC, ITEMS>;
-  const size_t smem = (size_t)p.stages * ((size_t)NC * ITEMS * sizeof(T) + 1024) + 1024;
+  const size_t smem = (size_t)p.stages * (p.stage_stride + NC * sizeof(unsigned long long)) + 1024;
   int rc = ensure_dynamic_smem((const void *)kfn, smem);
   if (rc) return rc;
-  const int threads = NC + 32 * kLookWarps + 32;
+  const int threads = pipe_threads(NC);
   if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
   const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
   kfn<<<grid, threads, smem, st>>>(tin, p);
@@ -772,7 +808,7 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   const size_t es = sizeof(T);
   const long long tile = (long long)block * items;
   const size_t stride = (size_t)tile * es + 1024;
-  const int stages = (int)std::min<size_t>(kMaxStages, kStageBudget / stride);
+  const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stride + block * sizeof(unsigned long long)));
   if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
@@ -782,7 +818,7 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   p.tail_begin = (unsigned long long)p.rows_full * epr;
   if (p.rows_full + tile / epr >= (1ll << 31)) return B2P_ERR_UNSUPPORTED;
   p.stages = stages;
-  p.lag = std::max(1, std::min(kMaxLag, stages - 3));
+  p.stage_stride = (unsigned)stride;
   p.in = in;
   p.out = out;
   p.hdr = reinterpret_cast<ScratchHeader *>(scratch);
@@ -799,7 +835,6 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   if (block == 128 && items == 32) return launch_copy_shape<T, 128, 32>(p, tin, st);
   if (block == 256 && items == 16) return launch_copy_shape<T, 256, 16>(p, tin, st);
   if (block == 256 && items == 32) return launch_copy_shape<T, 256, 32>(p, tin, st);
-  if (block == 512 && items == 16) return launch_copy_shape<T, 512, 16>(p, tin, st);
   return B2P_ERR_UNSUPPORTED;
 }
 
@@ -821,9 +856,8 @@ bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long ro
 
 bool scan_tma_shape(int dtype, int block, int items) {
   if (dtype == B2P_BF16 || dtype_size(dtype) == 0) return false;
-  const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) ||
-                     (block == 256 && items == 32) || (block == 512 && items == 16);
-  return shape && (size_t)block * items * dtype_size(dtype) * 3 <= kStageBudget;
+  const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) || (block == 256 && items == 32);
+  return shape && ((size_t)block * items * dtype_size(dtype) + (size_t)block * acc_size(dtype) * (dtype == B2P_F32 ? 2 : 1)) * 3 <= kSmemBudget;
 }
 
 int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out, size_t n, const void *init,
@@ -847,9 +881,8 @@ int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out,
 bool copy_if_tma_shape(int dtype, int block, int items) {
   const size_t es = dtype_size(dtype);
   if (es != 4 && es != 8) return false;
-  const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) ||
-                     (block == 256 && items == 32) || (block == 512 && items == 16);
-  return shape && ((size_t)block * items * es + 1024) * 3 <= kStageBudget;
+  const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) || (block == 256 && items == 32);
+  return shape && ((size_t)block * items * es + 1024 + (size_t)block * 8) * 3 <= kSmemBudget;
 }
 
 int launch_copy_if_tma(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs,

@@ -216,8 +216,9 @@ def test_scan_float_sum_vs_fp64(dev, code):
             assert np.max(np.abs(ge - ref_e) / ref_e) <= FLOAT_TOL, (n, cfg)
 
 
-# Pipelined (TMA) scan configurations: 128 x 32, 256 x 16, 256 x 32, 512 x 16.
-TMA_SCAN_CONFIGS = [19, 22, 23, 26]
+# Pipelined (TMA) scan configurations: 128 x 32, 256 x 16, 256 x 32 (512 x 16,
+# configuration 26, has no pipelined kernel and runs the two-phase kernel).
+TMA_SCAN_CONFIGS = [19, 22, 23]
 
 
 @pytest.mark.parametrize("code", [C.I32, C.I64, C.U32])
