@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
 // stores; the store warp writes the 16-byte-aligned middle with one bulk
 // copy.  Stages are 1024 bytes longer than a tile: packing may shift it by
 // up to 15 bytes.
-template <class T, int NC, int ITEMS>
+template <class T, int NC, int ITEMS, int CMP>
 __global__ void __launch_bounds__(pipe_threads(NC), 1)
     copy_if_tma_kernel(const __grid_constant__ CUtensorMap tin, TmaParams p) {
   constexpr int kTile = NC * ITEMS;
@@ -522,6 +522,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   extern __shared__ char smem_raw[];
   char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned long long *texcl_all = reinterpret_cast<unsigned long long *>(smem + (size_t)p.stages * p.stage_stride);
+  unsigned *keep_all = reinterpret_cast<unsigned *>(texcl_all + (size_t)p.stages * NC);
   __shared__ __align__(8) PipeState ps;
   __shared__ unsigned long long s_warp[32];
 
@@ -535,25 +536,32 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   const int ntail = (int)(p.n - p.tail_begin);
   T *out = reinterpret_cast<T *>(p.out);
 
-  // predicate flags of thread t's elements of a tile (the first `count`
-  // elements of the tile are real)
-  auto flags = [&](const char *buf, int t, int count, uint4 (&v)[VPT], int *kept) -> unsigned {
+  using U = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
+  const U mask = (U)p.mask, rhs = (U)p.rhs;
+  // predicate bits of thread t's elements of a tile (the first `count`
+  // elements of the tile are real); the comparison is a template argument
+  auto flags = [&](const char *buf, int t, int count, int *kept) -> unsigned {
     const int first = t * ITEMS;
     unsigned keep = 0;
-    int c = 0;
 #pragma unroll
     for (int k = 0; k < VPT; ++k) {
-      v[k] = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
-      const T *e = reinterpret_cast<const T *>(&v[k]);
+      const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+      const U *e = reinterpret_cast<const U *>(&w);
 #pragma unroll
       for (int qq = 0; qq < EPV; ++qq) {
-        const int j = k * EPV + qq;
-        const bool kb = (first + j < count) && pred_bits(e[qq], p.mask, p.cmp, p.rhs);
-        keep |= (unsigned)kb << j;
-        c += kb;
+        const U a = e[qq] & mask;
+        bool kb;
+        if constexpr (CMP == B2P_CMP_LT) kb = a < rhs;
+        else if constexpr (CMP == B2P_CMP_LE) kb = a <= rhs;
+        else if constexpr (CMP == B2P_CMP_EQ) kb = a == rhs;
+        else if constexpr (CMP == B2P_CMP_NE) kb = a != rhs;
+        else if constexpr (CMP == B2P_CMP_GE) kb = a >= rhs;
+        else kb = a > rhs;
+        keep |= (unsigned)kb << (k * EPV + qq);
       }
     }
-    *kept = c;
+    if (count < first + ITEMS) keep &= count <= first ? 0u : ((1u << (count - first)) - 1u);  // count - first < 32 here
+    *kept = __popc(keep);
     return keep;
   };
 
@@ -573,9 +581,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       char *buf = smem + (size_t)s * p.stage_stride;
       if (tile == last && ntail > 0) load_row_tail<T, NC>(p, buf, tile, kTile);
       const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
-      uint4 v[VPT];
       int kept;
-      (void)flags(buf, t, count, v, &kept);
+      keep_all[(size_t)s * NC + t] = flags(buf, t, count, &kept);
       unsigned long long tile_kept;
       texcl_all[(size_t)s * NC + t] =
           group_exclusive_scan<CountOps, NC>((unsigned long long)kept, s_warp, &tile_kept, t, 1);
@@ -608,23 +615,24 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         kept_total = 0;
       }
-      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
+      const unsigned keep = keep_all[(size_t)s * NC + t];
       uint4 v[VPT];
-      int kept;
-      const unsigned keep = flags(buf, t, count, v, &kept);
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) v[k] = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
       bar_named(2, NC);  // every emitter holds its elements: the stage may be overwritten
       const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
       const unsigned phase = (unsigned)(g0 & 15u);
-      unsigned long long o = texcl_all[(size_t)s * NC + t];
+      const unsigned o = (unsigned)texcl_all[(size_t)s * NC + t];
+      const unsigned lim = (unsigned)kept_total;
 #pragma unroll
       for (int k = 0; k < VPT; ++k) {
         const T *e = reinterpret_cast<const T *>(&v[k]);
 #pragma unroll
-        for (int qq = 0; qq < EPV; ++qq)
-          if (keep & (1u << (k * EPV + qq))) {
-            if (o < kept_total) *reinterpret_cast<T *>(buf + phase + o * sizeof(T)) = e[qq];
-            ++o;
-          }
+        for (int qq = 0; qq < EPV; ++qq) {
+          const int j = k * EPV + qq;
+          const unsigned pos = o + __popc(keep & ((1u << j) - 1u));
+          if (((keep >> j) & 1u) && pos < lim) *reinterpret_cast<T *>(buf + phase + pos * sizeof(T)) = e[qq];
+        }
       }
       fence_async_smem();
       bar_named(2, NC);
@@ -789,10 +797,10 @@ int dispatch(int op, int inclusive, const void *in, void *out, size_t n, const v
 #undef B2P_TMA_CASE
 }
 
-template <class T, int NC, int ITEMS>
+template <class T, int NC, int ITEMS, int CMP>
 int launch_copy_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
-  auto kfn = copy_if_tma_kernel<T, NC, ITEMS>;
-  const size_t smem = (size_t)p.stages * (p.stage_stride + NC * sizeof(unsigned long long)) + 1024;
+  auto kfn = copy_if_tma_kernel<T, NC, ITEMS, CMP>;
+  const size_t smem = (size_t)p.stages * (p.stage_stride + NC * (sizeof(unsigned long long) + 4)) + 1024;
   int rc = ensure_dynamic_smem((const void *)kfn, smem);
   if (rc) return rc;
   const int threads = pipe_threads(NC);
@@ -802,13 +810,33 @@ int launch_copy_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
+template <class T, int NC, int ITEMS>
+int launch_copy_items(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
+  switch (p.cmp) {
+  case B2P_CMP_LT: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_LT>(p, tin, st);
+  case B2P_CMP_LE: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_LE>(p, tin, st);
+  case B2P_CMP_EQ: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_EQ>(p, tin, st);
+  case B2P_CMP_NE: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_NE>(p, tin, st);
+  case B2P_CMP_GE: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_GE>(p, tin, st);
+  default: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_GT>(p, tin, st);
+  }
+}
+
+template <class T>
+int launch_copy_cmp(TmaParams &p, const CUtensorMap &tin, int block, int items, cudaStream_t st) {
+  if (block == 128 && items == 32) return launch_copy_items<T, 128, 32>(p, tin, st);
+  if (block == 256 && items == 16) return launch_copy_items<T, 256, 16>(p, tin, st);
+  if (block == 256 && items == 32) return launch_copy_items<T, 256, 32>(p, tin, st);
+  return B2P_ERR_UNSUPPORTED;
+}
+
 template <class T>
 int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs, uint64_t *num_copied,
                   void *scratch, int block, int items, cudaStream_t st) {
   const size_t es = sizeof(T);
   const long long tile = (long long)block * items;
   const size_t stride = (size_t)tile * es + 1024;
-  const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stride + block * sizeof(unsigned long long)));
+  const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stride + block * (sizeof(unsigned long long) + 4)));
   if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
@@ -832,10 +860,7 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   CUtensorMap tin;
   if (!encode_row_tensor(&tin, in, (unsigned long long)p.rows_full, (int)std::min<long long>(256, tile / epr)))
     return B2P_ERR_UNSUPPORTED;
-  if (block == 128 && items == 32) return launch_copy_shape<T, 128, 32>(p, tin, st);
-  if (block == 256 && items == 16) return launch_copy_shape<T, 256, 16>(p, tin, st);
-  if (block == 256 && items == 32) return launch_copy_shape<T, 256, 32>(p, tin, st);
-  return B2P_ERR_UNSUPPORTED;
+  return launch_copy_cmp<T>(p, tin, block, items, st);
 }
 
 }  // namespace
@@ -882,7 +907,7 @@ bool copy_if_tma_shape(int dtype, int block, int items) {
   const size_t es = dtype_size(dtype);
   if (es != 4 && es != 8) return false;
   const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) || (block == 256 && items == 32);
-  return shape && ((size_t)block * items * es + 1024 + (size_t)block * 8) * 3 <= kSmemBudget;
+  return shape && ((size_t)block * items * es + 1024 + (size_t)block * 12) * 3 <= kSmemBudget;
 }
 
 int launch_copy_if_tma(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs,

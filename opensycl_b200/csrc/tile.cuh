@@ -183,10 +183,24 @@ __device__ __forceinline__ void record_error(ScratchHeader *hdr, unsigned code) 
 // dedicated look-back warp polls without sleeping.
 constexpr int kLookW = 4;
 
+// W words per lane and step (W x 32 predecessors per L2 round trip).
+template <class Ops, int W, bool kBackoff>
+__device__ typename Ops::Pub lookback_w(const StatusWord *status, long long tile,
+                                        unsigned long long epoch_tag, unsigned long long timeout_ns,
+                                        bool &err);
+
 template <class Ops, bool kBackoff = true>
-__device__ typename Ops::Pub lookback(const StatusWord *status, long long tile,
-                                      unsigned long long epoch_tag, unsigned long long timeout_ns,
-                                      bool &err) {
+__device__ __forceinline__ typename Ops::Pub lookback(const StatusWord *status, long long tile,
+                                                      unsigned long long epoch_tag,
+                                                      unsigned long long timeout_ns, bool &err) {
+  return lookback_w<Ops, kLookW, kBackoff>(status, tile, epoch_tag, timeout_ns, err);
+}
+
+template <class Ops, int W, bool kBackoff>
+__device__ typename Ops::Pub lookback_w(const StatusWord *status, long long tile,
+                                        unsigned long long epoch_tag, unsigned long long timeout_ns,
+                                        bool &err) {
+  constexpr int kLookW = W;
   using Pub = typename Ops::Pub;
   const int lane = threadIdx.x & 31;
   Pub acc = Ops::identity();

@@ -53,7 +53,7 @@ int heuristic_config(int prim, int dtype, size_t n, int64_t nseg) {
       return cfg(1, 256, dtype_size(dtype) == 8 ? 16 : 32);
     return cfg(0, 256, dtype_size(dtype) == 8 ? 16 : 32);
   case B2P_PRIM_COPY_IF:
-    if (n * dtype_size(dtype) >= (8u << 20)) return cfg(1, 256, 16);
+    if (n * dtype_size(dtype) >= (8u << 20)) return cfg(1, 256, dtype_size(dtype) == 8 ? 16 : 32);
     return cfg(0, 256, dtype_size(dtype) == 8 ? 16 : 32);
   case B2P_PRIM_HISTOGRAM:
     return cfg(1, 1024, 32);
