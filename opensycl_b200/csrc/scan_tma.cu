@@ -47,8 +47,11 @@ constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
 struct TmaParams {
   unsigned long long n;
   long long ntiles;
-  long long rows_full;            // complete 128-byte rows (the tensor maps' extent)
-  unsigned long long tail_begin;  // first element past the complete rows
+  long long rows_full;            // complete 128-byte input rows (the input tensor map's extent)
+  unsigned long long tail_begin;  // first element past the complete input rows
+  long long rows_full_out;        // complete 128-byte output rows (scans)
+  unsigned long long tail_out_begin;  // first element past the complete output rows
+  unsigned out_offset;            // byte offset of a stage's output tile (0: in place)
   int inclusive;
   int has_init;
   unsigned long long init_raw;    // Out-typed init value
@@ -113,31 +116,40 @@ __device__ __forceinline__ typename P::Acc thread_total_t(const char *buf, int t
   return agg;
 }
 
-// fp32 SUM, reducer pass: compensated (TwoSum) running sums of the thread's
-// elements from zero, written back in place rounded to fp32 (inclusive:
-// after adding the element, exclusive: before).  Returns the thread total.
-template <int ITEMS, bool INCLUSIVE>
-__device__ __forceinline__ DF thread_runs_f32(char *buf, int t) {
-  constexpr int VPT = ITEMS / 4;
+// fp32 / bf16-input SUM, reducer pass: compensated (TwoSum) running sums of
+// the thread's elements from zero, rounded to fp32 and written to the
+// stage's output tile (in place for fp32 input; inclusive: after adding the
+// element, exclusive: before).  Returns the thread total.
+template <class In, int ITEMS, bool INCLUSIVE>
+__device__ __forceinline__ DF thread_runs(const char *inbuf, char *outbuf, int t) {
+  constexpr int IPV = 16 / (int)sizeof(In);
+  constexpr int VPT_IN = ITEMS / IPV, VPT_OUT = ITEMS / 4, OPI = IPV / 4;
   DF run{0.f, 0.f};
 #pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    float4 *slot = reinterpret_cast<float4 *>(buf + swz(t * VPT + k) * 16);
-    float4 w = *slot;
-    float *e = reinterpret_cast<float *>(&w);
+  for (int k = 0; k < VPT_IN; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT_IN + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&w);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if constexpr (INCLUSIVE) {
-        df_accumulate(run, e[q]);
-        e[q] = __fadd_rn(run.hi, run.lo);
-      } else {
-        const float before = __fadd_rn(run.hi, run.lo);
-        df_accumulate(run, e[q]);
-        e[q] = before;
+    for (int m = 0; m < OPI; ++m) {
+      float4 o;
+      float *oe = reinterpret_cast<float *>(&o);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float x;
+        if constexpr (sizeof(In) == 2) x = bf16_bits_to_f32(e[m * 4 + q]);
+        else x = e[m * 4 + q];
+        if constexpr (INCLUSIVE) {
+          df_accumulate(run, x);
+          oe[q] = __fadd_rn(run.hi, run.lo);
+        } else {
+          oe[q] = __fadd_rn(run.hi, run.lo);
+          df_accumulate(run, x);
+        }
       }
+      *reinterpret_cast<float4 *>(outbuf + swz(t * VPT_OUT + k * OPI + m) * 16) = o;
     }
-    *slot = w;
   }
+  (void)VPT_OUT;
   return df_norm(run);
 }
 
@@ -159,32 +171,37 @@ __device__ __forceinline__ void emit_f32_runs(char *buf, DF start, int t) {
   }
 }
 
-// Generic emitter pass: the thread's outputs from its running value, in place.
+// Generic emitter pass: the thread's outputs from its running value, into
+// the stage's output tile (in place when input and output sizes match; each
+// output vector overwrites only input this thread has already read).
 template <class P, int ITEMS>
-__device__ __forceinline__ void emit_generic(char *buf, typename P::Acc run, bool inclusive, int t) {
+__device__ __forceinline__ void emit_generic(const char *inbuf, char *outbuf, typename P::Acc run, bool inclusive,
+                                             int t) {
   using In = typename P::In;
   using Out = typename P::Out;
-  static_assert(sizeof(In) == sizeof(Out), "in place");
   constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
+  constexpr int OPV = 16 / (int)sizeof(Out);
+  constexpr int VPT_IN = ITEMS / IPV, VPT_OUT = ITEMS / OPV, OPI = IPV / OPV;
 #pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    uint4 *slot = reinterpret_cast<uint4 *>(buf + swz(t * VPT + k) * 16);
-    const uint4 w = *slot;
+  for (int k = 0; k < VPT_IN; ++k) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT_IN + k) * 16);
     const In *e = reinterpret_cast<const In *>(&w);
-    uint4 o;
-    Out *oe = reinterpret_cast<Out *>(&o);
 #pragma unroll
-    for (int q = 0; q < IPV; ++q) {
-      if (inclusive) {
-        P::add(run, e[q]);
-        oe[q] = P::finalize(run);
-      } else {
-        oe[q] = P::finalize(run);
-        P::add(run, e[q]);
+    for (int m = 0; m < OPI; ++m) {
+      uint4 o;
+      Out *oe = reinterpret_cast<Out *>(&o);
+#pragma unroll
+      for (int q = 0; q < OPV; ++q) {
+        if (inclusive) {
+          P::add(run, e[m * OPV + q]);
+          oe[q] = P::finalize(run);
+        } else {
+          oe[q] = P::finalize(run);
+          P::add(run, e[m * OPV + q]);
+        }
       }
+      *reinterpret_cast<uint4 *>(outbuf + swz(t * VPT_OUT + k * OPI + m) * 16) = o;
     }
-    *slot = o;
   }
 }
 
@@ -377,14 +394,17 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   using Acc = typename P::Acc;
   using Out = typename P::Out;
   using Ops = typename std::conditional<WIDE, F64Ops, AccOps<P>>::type;
-  static_assert(sizeof(In) == sizeof(Out), "in-place emission needs equal element sizes");
+  static_assert(sizeof(Out) == sizeof(In) || sizeof(Out) == 2 * sizeof(In), "output tile layout");
   constexpr int kTile = NC * ITEMS;
-  constexpr int kEpr = 128 / (int)sizeof(In);  // elements per 128-byte row
-  static_assert(kTile % (8 * kEpr) == 0, "a stage is a whole number of 1024-byte swizzle atoms");
-  constexpr int kRows = kTile / kEpr;
-  constexpr int kBox = kRows < 256 ? kRows : 256;
-  static_assert(kRows % kBox == 0, "box rows");
-  constexpr bool kFast = std::is_same<P, FloatSumPolicy<float>>::value;
+  constexpr int kEpr = 128 / (int)sizeof(In);      // input elements per 128-byte row
+  constexpr int kEprOut = 128 / (int)sizeof(Out);  // output elements per 128-byte row
+  static_assert(kTile % (8 * kEpr) == 0 && kTile % (8 * kEprOut) == 0,
+                "input and output tiles are whole numbers of 1024-byte swizzle atoms");
+  constexpr int kRows = kTile / kEpr, kRowsOut = kTile / kEprOut;
+  constexpr int kBox = kRows < 256 ? kRows : 256, kBoxOut = kRowsOut < 256 ? kRowsOut : 256;
+  static_assert(kRows % kBox == 0 && kRowsOut % kBoxOut == 0, "box rows");
+  // fp32 and bf16-input SUM keep compensated runs in the output tile
+  constexpr bool kFast = std::is_same<P, FloatSumPolicy<float>>::value || std::is_same<P, FloatSumPolicy<uint16_t>>::value;
 
   extern __shared__ char smem_raw[];
   char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -402,6 +422,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   const int S = p.stages;
   const long long last = p.ntiles - 1;
   const int ntail = (int)(p.n - p.tail_begin);
+  const int ntail_out = (int)(p.n - p.tail_out_begin);
 
   if (warp < NC / 32) {
     // ------------------------------------------------------------ reducers
@@ -419,7 +440,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       char *buf = smem + (size_t)s * p.stage_stride;
       if (tile == last && ntail > 0) load_row_tail<In, NC>(p, buf, tile, kTile);
       Acc agg;
-      if constexpr (kFast) agg = p.inclusive ? thread_runs_f32<ITEMS, true>(buf, t) : thread_runs_f32<ITEMS, false>(buf, t);
+      if constexpr (kFast)
+        agg = p.inclusive ? thread_runs<In, ITEMS, true>(buf, buf + p.out_offset, t)
+                          : thread_runs<In, ITEMS, false>(buf, buf + p.out_offset, t);
       else agg = thread_total_t<P, ITEMS>(buf, t);
       Acc tile_agg;
       texcl_all[(size_t)s * NC + t] = group_exclusive_scan<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
@@ -453,14 +476,15 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       const int s = r.s;
       const long long tile = ps.tile[s];
       char *buf = smem + (size_t)s * p.stage_stride;
+      char *obuf = buf + p.out_offset;
       const Acc start = start_value<P, WIDE>(ps.carry[s], texcl_all[(size_t)s * NC + t]);
-      if constexpr (kFast) emit_f32_runs<ITEMS>(buf, start, t);
-      else emit_generic<P, ITEMS>(buf, start, p.inclusive != 0, t);
+      if constexpr (kFast) emit_f32_runs<ITEMS>(obuf, start, t);
+      else emit_generic<P, ITEMS>(buf, obuf, start, p.inclusive != 0, t);
       fence_async_smem();
       bar_named(2, NC);
-      if (tile == last && ntail > 0) {
-        const long long j0 = (long long)p.tail_begin - tile * kTile;
-        if (t < ntail) out[p.tail_begin + t] = *smem_elem_ptr<Out>(buf, (int)j0 + t);
+      if (tile == last && ntail_out > 0) {
+        const long long j0 = (long long)p.tail_out_begin - tile * kTile;
+        if (t < ntail_out) out[p.tail_out_begin + t] = *smem_elem_ptr<Out>(obuf, (int)j0 + t);
         bar_named(2, NC);
       }
       if (t == 0) mbar_arrive(&ps.emitted[s]);
@@ -483,10 +507,10 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         }
         if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
         const long long tile = ps.tile[s];
-        const long long r0 = tile * kRows;
-        const long long rows_out = min((long long)kRows, p.rows_full - r0);
-        for (long long rr = 0; rr < rows_out; rr += kBox)
-          tma_store_2d(&tout, 0, (int)(r0 + rr), smem + (size_t)s * p.stage_stride + rr * 128, spol);
+        const long long r0 = tile * kRowsOut;
+        const long long rows_out = min((long long)kRowsOut, p.rows_full_out - r0);
+        for (long long rr = 0; rr < rows_out; rr += kBoxOut)
+          tma_store_2d(&tout, 0, (int)(r0 + rr), smem + (size_t)s * p.stage_stride + p.out_offset + rr * 128, spol);
         bulk_commit();
         bulk_wait_read<0>();
         mbar_arrive(&ps.empty[s]);
@@ -736,18 +760,24 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
              int block, int items, cudaStream_t st) {
   using In = typename P::In;
   using Out = typename P::Out;
-  const size_t es = sizeof(In);
+  const size_t es = sizeof(In), eo = sizeof(Out);
   const long long tile = (long long)block * items;
-  const size_t stage = (size_t)tile * es;
+  // a stage holds the input tile, and after it the output tile when the
+  // output element is wider (bf16 in, fp32 out)
+  const size_t in_bytes = (size_t)tile * es;
+  const size_t stage = in_bytes + (eo != es ? (size_t)tile * eo : 0);
   const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stage + block * sizeof(typename P::Acc)));
   if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
   p.ntiles = (long long)((n + tile - 1) / tile);
-  const long long epr = 128 / (long long)es;
+  const long long epr = 128 / (long long)es, epr_out = 128 / (long long)eo;
   p.rows_full = (long long)(n / (size_t)epr);
   p.tail_begin = (unsigned long long)p.rows_full * epr;
-  if (p.rows_full + tile / epr >= (1ll << 31)) return B2P_ERR_UNSUPPORTED;
+  p.rows_full_out = (long long)(n / (size_t)epr_out);
+  p.tail_out_begin = (unsigned long long)p.rows_full_out * epr_out;
+  if (p.rows_full_out + tile / epr_out >= (1ll << 31)) return B2P_ERR_UNSUPPORTED;
+  p.out_offset = eo != es ? (unsigned)in_bytes : 0u;
   p.inclusive = inclusive;
   p.stages = stages;
   p.stage_stride = (unsigned)stage;
@@ -761,9 +791,9 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
   p.has_init = init != nullptr;
   if (init) memcpy(&p.init_raw, init, sizeof(Out));
   CUtensorMap tin, tout;
-  const int box = (int)std::min<long long>(256, tile / epr);
-  if (!encode_row_tensor(&tin, in, (unsigned long long)p.rows_full, box) ||
-      !encode_row_tensor(&tout, out, (unsigned long long)p.rows_full, box))
+  if (!encode_row_tensor(&tin, in, (unsigned long long)p.rows_full, (int)std::min<long long>(256, tile / epr)) ||
+      !encode_row_tensor(&tout, out, (unsigned long long)p.rows_full_out,
+                         (int)std::min<long long>(256, tile / epr_out)))
     return B2P_ERR_UNSUPPORTED;
   if constexpr (P::kCompensated) {
     if (wide) return launch_policy<P, true>(p, tin, tout, block, items, st);
@@ -784,7 +814,7 @@ int dispatch(int op, int inclusive, const void *in, void *out, size_t n, const v
     B2P_TMA_CASE(B2P_MAX)
   default: break;
   }
-  if constexpr (DT == B2P_F32 || DT == B2P_F64) {
+  if constexpr (DT == B2P_F32 || DT == B2P_F64 || DT == B2P_BF16) {
     return B2P_ERR_UNSUPPORTED;
   } else {
     switch (op) {
@@ -880,9 +910,12 @@ bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long ro
 }
 
 bool scan_tma_shape(int dtype, int block, int items) {
-  if (dtype == B2P_BF16 || dtype_size(dtype) == 0) return false;
+  if (dtype_size(dtype) == 0) return false;
   const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) || (block == 256 && items == 32);
-  return shape && ((size_t)block * items * dtype_size(dtype) + (size_t)block * acc_size(dtype) * (dtype == B2P_F32 ? 2 : 1)) * 3 <= kSmemBudget;
+  const size_t es = dtype_size(dtype), eo = acc_size(dtype);
+  const size_t stage = (size_t)block * items * (es + (eo != es ? eo : 0));
+  const size_t acc = dtype_is_float(dtype) && dtype != B2P_F64 ? 8 : acc_size(dtype);
+  return shape && (stage + (size_t)block * acc) * 3 <= kSmemBudget;
 }
 
 int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out, size_t n, const void *init,
@@ -899,6 +932,7 @@ int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out,
   case B2P_U64: return dispatch<B2P_U64>(op, inclusive, in, out, n, init, scratch, block, items, st);
   case B2P_F32: return dispatch<B2P_F32>(op, inclusive, in, out, n, init, scratch, block, items, st);
   case B2P_F64: return dispatch<B2P_F64>(op, inclusive, in, out, n, init, scratch, block, items, st);
+  case B2P_BF16: return dispatch<B2P_BF16>(op, inclusive, in, out, n, init, scratch, block, items, st);
   default: return B2P_ERR_UNSUPPORTED;
   }
 }

@@ -243,6 +243,30 @@ def test_scan_pipelined_row_tails(dev, code):
                                   O.scan(code, C.SUM, False, x, init)), (cfg, n)
 
 
+def test_scan_pipelined_bf16_in_fp32_out(dev):
+    """bf16 input, fp32 output through the pipelined kernel (the output tile
+    sits beside the input tile in each stage): SUM against FP64, MAX exact,
+    around 64-element input rows and 32-element output rows."""
+    rng = np.random.default_rng(570)
+    for cfg in TMA_SCAN_CONFIGS:
+        blk, items = C.config_describe(cfg)[:2]
+        tile = blk * items
+        for n in [tile, 2 * tile + 63, 3 * tile + 32 * 5 + 7, 5 * tile + tile // 2 + 1]:
+            x = rand_floats(rng, C.BF16, n, positive=True)
+            xd = to_dev(x, C.BF16)
+            ref_i = O.fp64_scan(C.BF16, True, x, 0.0)
+            ref_e = O.fp64_scan(C.BF16, False, x, 1.5)
+            gi = to_np(C.scan(xd, True, "sum", None, config=cfg)).astype(np.float64)
+            ge = to_np(C.scan(xd, False, "sum", 1.5, config=cfg)).astype(np.float64)
+            pos = ref_i > 0
+            assert np.max(np.abs(gi - ref_i)[pos] / ref_i[pos]) <= FLOAT_TOL, (cfg, n)
+            assert np.max(np.abs(ge - ref_e) / ref_e) <= FLOAT_TOL, (cfg, n)
+            xs = O.bf16_to_f32(rand_floats(rng, C.BF16, n))
+            xsd = to_dev(O.bf16_round(xs), C.BF16)
+            gm = to_np(C.scan(xsd, True, C.MAX, None, config=cfg))
+            assert np.array_equal(gm, np.maximum.accumulate(xs).astype(np.float32)), (cfg, n)
+
+
 def test_scan_pipelined_fp32_long_exclusive(dev):
     """fp32 SUM longer than 2^24 (FP64 tile carries) through the pipelined
     kernel, inclusive and exclusive with init."""
