@@ -28,6 +28,7 @@
 // header and the block leaves its loops.
 #include "scan_tile.cuh"
 #include "tma.cuh"
+#include "tmem.cuh"
 #include "internal.h"
 
 #include <algorithm>
@@ -37,9 +38,19 @@ namespace b2p {
 
 namespace {
 
-constexpr int kMaxStages = 12;
+constexpr int kMaxStages = 16;
 constexpr int kLookWarps = 2;
+// Bulk stores a store warp keeps in flight before it waits for the oldest
+// one to finish reading its stage (2 and 3 measured slower: a stage held by
+// a store is a stage the producer cannot fill).
+constexpr int kStoresInFlight = 1;
+// Fewest stages a pipelined launch runs with.
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int kMinStages = cmax(3, cmax(kLookWarps, kStoresInFlight));
 constexpr size_t kSmemBudget = 210 * 1024;  // stages + thread prefixes
+// Scans stage tiles that wait for their carries in TMEM where the policy
+// and shape allow it.
+constexpr bool kUseTmem = true;
 
 // Threads of a pipelined block with NC reducer and NC emitter threads.
 constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
@@ -57,6 +68,13 @@ struct TmaParams {
   unsigned long long init_raw;    // Out-typed init value
   int stages;
   unsigned stage_stride;          // bytes between stages
+  // TMEM-staged scan: carry slots in TMEM, output stages after the input
+  // stages, thread prefixes per slot after the output stages
+  int slots;
+  int out_stages;
+  unsigned out_stage_stride;
+  unsigned out_base;
+  unsigned texcl_base;
   const void *in;
   void *out;
   ScratchHeader *hdr;
@@ -77,6 +95,11 @@ struct TmaParams {
 struct PipeState {
   uint64_t full[kMaxStages], empty[kMaxStages], aggr[kMaxStages], cready[kMaxStages], emitted[kMaxStages];
   long long tile[kMaxStages];
+  // TMEM-staged scan: slot handed back by the emitters, output stage handed
+  // back by the store warp, tile ids of input and output stages, TMEM base
+  uint64_t slot_free[kMaxStages], out_empty[kMaxStages];
+  long long tile_in[kMaxStages], tile_out[kMaxStages];
+  uint32_t tmem_base;
   unsigned long long agg[kMaxStages], carry[kMaxStages];
   unsigned long long epoch;
   long long end_item;  // number of tiles this block handles, once the reducers know it
@@ -273,7 +296,7 @@ __device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
 // in boxes of `box` rows.  A tile wholly past the complete rows completes
 // its stage without a copy.  Tile id -1 ends the reducers.
 __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaParams &p, PipeState &ps,
-                                              char *smem, int rows, int box) {
+                                              char *smem, int rows, int box, long long *tiles) {
   prefetch_tensormap(tin);
   const unsigned long long pol = l2_policy_stream();
   const int S = p.stages;
@@ -281,17 +304,17 @@ __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaP
     const int s = r.s;
     if (!mbar_wait(&ps.empty[s], r.ph ^ 1u, p.timeout_ns)) {
       record_error(p.hdr, B2P_ERR_TIMEOUT);
-      ps.tile[s] = -1;
+      tiles[s] = -1;
       mbar_arrive(&ps.full[s]);
       return;
     }
     const long long tile = (long long)atomicAdd(&p.hdr->tile_ctr, 1ull);
     if (tile >= p.ntiles) {
-      ps.tile[s] = -1;
+      tiles[s] = -1;
       mbar_arrive(&ps.full[s]);
       return;
     }
-    ps.tile[s] = tile;
+    tiles[s] = tile;
     const long long r0 = tile * rows;
     const long long rows_in = min((long long)rows, p.rows_full - r0);
     const int nbox = rows_in > 0 ? (int)((rows_in + box - 1) / box) : 0;
@@ -311,10 +334,9 @@ __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaP
 // and hands the carry to the emitters.
 template <class Ops>
 __device__ __forceinline__ void lookback_loop(const TmaParams &p, PipeState &ps, int wi,
-                                              unsigned long long init_bits, unsigned long long epoch_tag) {
+                                              unsigned long long init_bits, unsigned long long epoch_tag, int S) {
   using Pub = typename Ops::Pub;
   const int lane = threadIdx.x & 31;
-  const int S = p.stages;
   RingPos r;
   r.advance(wi, S);
   for (long long it = wi;; it += kLookWarps, r.advance(kLookWarps, S)) {
@@ -371,6 +393,25 @@ __device__ __forceinline__ void emitters_finish(const TmaParams &p, PipeState &p
   mbar_arrive(&ps.emitted[r.s]);
   for (int j = 0; j < kLookWarps; ++j, r.advance(1, p.stages)) mbar_arrive(&ps.aggr[r.s]);
 }
+
+// Store warp: stages whose bulk stores were committed but may still read
+// shared memory.  A stage is handed back to the producer (empty barrier)
+// once its store has read it; up to kStoresInFlight stores overlap.
+struct StoreRelease {
+  RingPos oldest;
+  int pending = 0;
+  __device__ __forceinline__ void committed(PipeState &ps, int S) {
+    if (++pending < kStoresInFlight) return;
+    bulk_wait_read<kStoresInFlight - 1>();
+    mbar_arrive(&ps.empty[oldest.s]);
+    oldest.advance(1, S);
+    --pending;
+  }
+  __device__ __forceinline__ void drain(PipeState &ps, int S) {
+    bulk_wait_read<0>();
+    for (; pending > 0; --pending, oldest.advance(1, S)) mbar_arrive(&ps.empty[oldest.s]);
+  }
+};
 
 // Elements past the complete rows (only in the last tile) into the stage,
 // by the reducer group (threads 0 .. ntail-1 of the block).
@@ -490,15 +531,16 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       if (t == 0) mbar_arrive(&ps.emitted[s]);
     }
   } else if (warp < 2 * NC / 32 + kLookWarps) {
-    lookback_loop<Ops>(p, ps, warp - 2 * NC / 32, init_bits, epoch_tag);
+    lookback_loop<Ops>(p, ps, warp - 2 * NC / 32, init_bits, epoch_tag, S);
   } else if (warp == 2 * NC / 32 + kLookWarps) {
-    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox);
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile);
   } else {
     // ---------------------------------------------------------- store warp
     if ((threadIdx.x & 31) == 0) {
       prefetch_tensormap(&tout);
       const unsigned long long spol = l2_policy_stream();
       RingPos r;
+      StoreRelease rel;
       for (long long it = 0;; ++it, r.advance(1, S)) {
         const int s = r.s;
         if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
@@ -512,11 +554,302 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         for (long long rr = 0; rr < rows_out; rr += kBoxOut)
           tma_store_2d(&tout, 0, (int)(r0 + rr), smem + (size_t)s * p.stage_stride + p.out_offset + rr * 128, spol);
         bulk_commit();
+        rel.committed(ps, S);
+      }
+      rel.drain(ps, S);
+      bulk_wait_all();
+    }
+  }
+  finish_launch(p.hdr, epoch, nullptr, 0);
+}
+
+// ------------------------------------------------------ scan, TMEM-staged
+//
+// The same roles as scan_tma_kernel, with a third place for a tile to wait:
+// reducers read a landed tile into registers, hand the input stage straight
+// back to the producer, and park the tile's running values in a TMEM slot
+// (32-bit cells: thread t of the reducer group owns lane 32 (w % 4) + t % 32
+// of its warp w and kCols consecutive columns of the slot).  Emitters take a
+// slot once its carry is known, add the carry and write the outputs into a
+// separate output stage for the store warp.  Shared memory then only holds
+// tiles on their way in and out, while up to 512 / kSlotCols tiles wait for
+// their carries in TMEM.
+
+// Policies whose outputs the TMEM kernel forms as combine(start, run) with
+// the bits of the in-place kernel's sequential pass: integer operators (exact
+// in wrap-around arithmetic) and fp32 / bf16-input SUM (the same
+// start.hi + (start.lo + run) formula).  Floating-point PROD, MIN, MAX and
+// fp64 SUM stay on the in-place kernel.
+template <class P>
+struct TmemExact : std::integral_constant<bool, P::kCompensated || std::is_integral<typename P::Acc>::value> {};
+
+// TMEM columns a reducer thread fills per tile.
+template <class P, int ITEMS>
+constexpr int tmem_cols() {
+  return ITEMS * (int)sizeof(typename P::Out) / 4;
+}
+
+// Reducer pass: the thread's ITEMS elements from the landed stage, their
+// running values from the identity (inclusive: after adding the element,
+// exclusive: before) as 32-bit words for TMEM, and the thread total.
+template <class P, int ITEMS, bool INCL>
+__device__ __forceinline__ typename P::Acc tmem_runs(const char *inbuf, uint32_t *w, int t) {
+  using In = typename P::In;
+  using Out = typename P::Out;
+  constexpr int IPV = 16 / (int)sizeof(In), VPT = ITEMS / IPV, WPO = (int)sizeof(Out) / 4;
+  typename P::Acc run = P::identity();
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT + k) * 16);
+    const In *e = reinterpret_cast<const In *>(&u);
+#pragma unroll
+    for (int q = 0; q < IPV; ++q) {
+      Out o;
+      if constexpr (P::kCompensated) {
+        const float x = P::lift_f(e[q]);
+        if constexpr (INCL) {
+          df_accumulate(run, x);
+          o = __fadd_rn(run.hi, run.lo);
+        } else {
+          o = __fadd_rn(run.hi, run.lo);
+          df_accumulate(run, x);
+        }
+      } else {
+        if constexpr (INCL) {
+          P::add(run, e[q]);
+          o = P::finalize(run);
+        } else {
+          o = P::finalize(run);
+          P::add(run, e[q]);
+        }
+      }
+      memcpy(w + (k * IPV + q) * WPO, &o, sizeof(Out));
+    }
+  }
+  if constexpr (P::kCompensated) run = df_norm(run);
+  return run;
+}
+
+// Emitter pass: outputs = start combined with the parked running values,
+// written to the output stage in the swizzled layout.
+template <class P, int ITEMS>
+__device__ __forceinline__ void tmem_emit(const uint32_t *w, typename P::Acc start, char *obuf, int t) {
+  using Out = typename P::Out;
+  constexpr int OPV = 16 / (int)sizeof(Out), VPT = ITEMS / OPV, WPO = (int)sizeof(Out) / 4;
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    uint4 u;
+    Out *oe = reinterpret_cast<Out *>(&u);
+#pragma unroll
+    for (int q = 0; q < OPV; ++q) {
+      Out r;
+      memcpy(&r, w + (k * OPV + q) * WPO, sizeof(Out));
+      if constexpr (P::kCompensated) oe[q] = __fadd_rn(start.hi, __fadd_rn(start.lo, r));
+      else oe[q] = P::finalize(P::combine(start, P::from_out(r)));
+    }
+    *reinterpret_cast<uint4 *>(obuf + swz(t * VPT + k) * 16) = u;
+  }
+}
+
+// Thread 0: barriers of the three rings (input stages, TMEM slots, output
+// stages) and the launch epoch.  Reducer and emitter warps arrive one by one
+// on the barriers that hand back input stages and slots.
+__device__ __forceinline__ void tmem_pipe_init(PipeState &ps, const TmaParams &p, unsigned group_warps) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < p.stages; ++i) {
+      mbar_init(&ps.full[i], 1);
+      mbar_init(&ps.empty[i], group_warps);
+    }
+    for (int i = 0; i < p.slots; ++i) {
+      mbar_init(&ps.aggr[i], 1);
+      mbar_init(&ps.cready[i], 1);
+      mbar_init(&ps.slot_free[i], group_warps);
+    }
+    for (int i = 0; i < p.out_stages; ++i) {
+      mbar_init(&ps.emitted[i], 1);
+      mbar_init(&ps.out_empty[i], 1);
+    }
+    mbar_init_fence();
+    ps.epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
+    ps.end_item = 0x7fffffffffffffffll;
+  }
+}
+
+template <class P, int NC, int ITEMS, bool WIDE>
+__global__ void __launch_bounds__(pipe_threads(NC), 1)
+    scan_tmem_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
+                     TmaParams p) {
+  using In = typename P::In;
+  using Acc = typename P::Acc;
+  using Out = typename P::Out;
+  using Ops = typename std::conditional<WIDE, F64Ops, AccOps<P>>::type;
+  constexpr int kTile = NC * ITEMS;
+  constexpr int kEpr = 128 / (int)sizeof(In), kEprOut = 128 / (int)sizeof(Out);
+  static_assert(kTile % (8 * kEpr) == 0 && kTile % (8 * kEprOut) == 0,
+                "input and output tiles are whole numbers of 1024-byte swizzle atoms");
+  constexpr int kRows = kTile / kEpr, kRowsOut = kTile / kEprOut;
+  constexpr int kBox = kRows < 256 ? kRows : 256, kBoxOut = kRowsOut < 256 ? kRowsOut : 256;
+  static_assert(kRows % kBox == 0 && kRowsOut % kBoxOut == 0, "box rows");
+  constexpr int kCols = tmem_cols<P, ITEMS>();
+  static_assert(kCols == 16 || kCols == 32, "TMEM columns per thread");
+  static_assert(NC % 128 == 0, "reducer and emitter groups cover the four TMEM lane quarters evenly");
+  constexpr int kSlotCols = kCols * (NC / 128);
+
+  extern __shared__ char smem_raw[];
+  char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  char *obase = smem + p.out_base;
+  Acc *texcl_all = reinterpret_cast<Acc *>(smem + p.texcl_base);
+  __shared__ __align__(8) PipeState ps;
+  __shared__ Acc s_warp[32];
+  __shared__ int s_go[2];
+
+  const int warp = threadIdx.x >> 5;
+  tmem_pipe_init(ps, p, NC / 32);
+  if (warp == 0) {
+    __syncwarp();
+    tmem_alloc(&ps.tmem_base, 512);
+  }
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tbase = ps.tmem_base;
+  const unsigned long long epoch = ps.epoch;
+  const unsigned long long epoch_tag = epoch << 8;
+  const unsigned long long init_bits = tile0_carry<P, WIDE>(p);
+  const int SI = p.stages, SL = p.slots, SO = p.out_stages;
+  const long long last = p.ntiles - 1;
+  const int ntail = (int)(p.n - p.tail_begin);
+  const int ntail_out = (int)(p.n - p.tail_out_begin);
+
+  if (warp < NC / 32) {
+    // ------------------------------------------------------------ reducers
+    // The group leader waits (bounded) and shares the outcome, so that the
+    // group always takes the same branch.
+    const int t = threadIdx.x;
+    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * kCols);
+    long long it = 0;
+    RingPos ri, rs;
+    for (;; ++it, ri.advance(1, SI), rs.advance(1, SL)) {
+      if (t == 0) {
+        int go = mbar_wait(&ps.full[ri.s], ri.ph, p.timeout_ns) ? 1 : -1;
+        if (go > 0 && ps.tile_in[ri.s] < 0) go = 0;
+        if (go > 0 && !mbar_wait(&ps.slot_free[rs.s], rs.ph ^ 1u, p.timeout_ns)) go = -1;
+        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        s_go[0] = go;
+      }
+      bar_named(1, NC);
+      if (s_go[0] <= 0) break;
+      (void)mbar_try(&ps.full[ri.s], ri.ph);  // completed: this thread's acquire of the TMA bytes
+      tmem_fence_after();
+      const long long tile = ps.tile_in[ri.s];
+      char *buf = smem + (size_t)ri.s * p.stage_stride;
+      if (tile == last && ntail > 0) load_row_tail<In, NC>(p, buf, tile, kTile);
+      uint32_t w[kCols];
+      const Acc agg = p.inclusive ? tmem_runs<P, ITEMS, true>(buf, w, t) : tmem_runs<P, ITEMS, false>(buf, w, t);
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.empty[ri.s]);  // this warp is done with the input stage
+      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
+      tmem_st16(ta, w);
+      if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
+      Acc tile_agg;
+      texcl_all[(size_t)rs.s * NC + t] = group_exclusive_scan<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
+      tmem_wait_st();
+      tmem_fence_before();
+      bar_named(1, NC);  // slot and thread prefixes complete
+      if (t == 0) {
+        const unsigned long long bits = publish_value<P, WIDE>(tile_agg);
+        if (tile != p.stall_tile) {
+          if (tile == 0)
+            st_status(p.status, Ops::pack(Ops::combine(Ops::unpack(init_bits), Ops::unpack(bits))),
+                      epoch_tag | kFlagPrefix);
+          else
+            st_status(p.status + tile, bits, epoch_tag | kFlagAgg);
+        }
+        ps.tile[rs.s] = tile;
+        ps.agg[rs.s] = bits;
+        mbar_arrive(&ps.aggr[rs.s]);
+      }
+    }
+    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
+  } else if (warp < 2 * NC / 32) {
+    // ------------------------------------------------------------ emitters
+    const int t = threadIdx.x - NC;
+    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(((t >> 5) >> 2) * kCols);
+    Out *out = reinterpret_cast<Out *>(p.out);
+    RingPos rs, ro;
+    for (long long it = 0;; ++it, rs.advance(1, SL), ro.advance(1, SO)) {
+      if (t == 0) {
+        int go = emitter_wait(p, ps, rs, it);
+        if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
+        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        if (go == 0) {
+          // every earlier item passed the look-back warps and the store warp:
+          // end them (look-back warps wait on items it .. it + kLookWarps - 1)
+          mbar_arrive(&ps.emitted[ro.s]);
+          RingPos r = rs;
+          for (int j = 0; j < kLookWarps; ++j, r.advance(1, SL)) mbar_arrive(&ps.aggr[r.s]);
+        }
+        s_go[1] = go;
+      }
+      bar_named(2, NC);
+      if (s_go[1] <= 0) break;
+      tmem_fence_after();
+      const long long tile = ps.tile[rs.s];
+      uint32_t w[kCols];
+      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
+      if constexpr (kCols == 32) tmem_load32(ta, w);
+      else tmem_load16(ta, w);
+      const Acc start = start_value<P, WIDE>(ps.carry[rs.s], texcl_all[(size_t)rs.s * NC + t]);
+      tmem_fence_before();
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.slot_free[rs.s]);  // slot, carry and prefixes read
+      char *obuf = obase + (size_t)ro.s * p.out_stage_stride;
+      tmem_emit<P, ITEMS>(w, start, obuf, t);
+      fence_async_smem();
+      bar_named(2, NC);
+      if (tile == last && ntail_out > 0) {
+        const long long j0 = (long long)p.tail_out_begin - tile * kTile;
+        if (t < ntail_out) out[p.tail_out_begin + t] = *smem_elem_ptr<Out>(obuf, (int)j0 + t);
+        bar_named(2, NC);
+      }
+      if (t == 0) {
+        ps.tile_out[ro.s] = tile;
+        mbar_arrive(&ps.emitted[ro.s]);
+      }
+    }
+  } else if (warp < 2 * NC / 32 + kLookWarps) {
+    lookback_loop<Ops>(p, ps, warp - 2 * NC / 32, init_bits, epoch_tag, SL);
+  } else if (warp == 2 * NC / 32 + kLookWarps) {
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile_in);
+  } else {
+    // ---------------------------------------------------------- store warp
+    if ((threadIdx.x & 31) == 0) {
+      prefetch_tensormap(&tout);
+      const unsigned long long spol = l2_policy_stream();
+      RingPos ro;
+      for (long long it = 0;; ++it, ro.advance(1, SO)) {
+        if (!mbar_wait(&ps.emitted[ro.s], ro.ph, p.timeout_ns)) {
+          record_error(p.hdr, B2P_ERR_TIMEOUT);
+          break;
+        }
+        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+        const long long tile = ps.tile_out[ro.s];
+        const long long r0 = tile * kRowsOut;
+        const long long rows_out = min((long long)kRowsOut, p.rows_full_out - r0);
+        const char *src = obase + (size_t)ro.s * p.out_stage_stride;
+        for (long long rr = 0; rr < rows_out; rr += kBoxOut) tma_store_2d(&tout, 0, (int)(r0 + rr), src + rr * 128, spol);
+        bulk_commit();
         bulk_wait_read<0>();
-        mbar_arrive(&ps.empty[s]);
+        mbar_arrive(&ps.out_empty[ro.s]);
       }
       bulk_wait_all();
     }
+  }
+  tmem_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(tbase, 512);
   }
   finish_launch(p.hdr, epoch, nullptr, 0);
 }
@@ -676,13 +1009,14 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       if (t == 0) mbar_arrive(&ps.emitted[s]);
     }
   } else if (warp < 2 * NC / 32 + kLookWarps) {
-    lookback_loop<CountOps>(p, ps, warp - 2 * NC / 32, 0ull, epoch_tag);
+    lookback_loop<CountOps>(p, ps, warp - 2 * NC / 32, 0ull, epoch_tag, S);
   } else if (warp == 2 * NC / 32 + kLookWarps) {
-    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox);
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile);
   } else {
     // ---------------------------------------------------------- store warp
     if ((threadIdx.x & 31) == 0) {
       RingPos r;
+      StoreRelease rel;
       for (long long it = 0;; ++it, r.advance(1, S)) {
         const int s = r.s;
         if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
@@ -703,9 +1037,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
                        : "memory");
         }
         bulk_commit();
-        bulk_wait_read<0>();
-        mbar_arrive(&ps.empty[s]);
+        rel.committed(ps, S);
       }
+      rel.drain(ps, S);
       bulk_wait_all();
     }
   }
@@ -746,6 +1080,58 @@ int launch_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, 
   return cuda_status(cudaGetLastError());
 }
 
+template <class P, int NC, int ITEMS, bool WIDE>
+int launch_tmem_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, cudaStream_t st) {
+  constexpr int cols = tmem_cols<P, ITEMS>();
+  if constexpr (!TmemExact<P>::value || (cols != 16 && cols != 32)) {
+    return B2P_ERR_UNSUPPORTED;
+  } else {
+    auto kfn = scan_tmem_kernel<P, NC, ITEMS, WIDE>;
+    const size_t smem = p.texcl_base + (size_t)p.slots * NC * sizeof(typename P::Acc) + 1024;
+    int rc = ensure_dynamic_smem((const void *)kfn, smem);
+    if (rc) return rc;
+    const int threads = pipe_threads(NC);
+    if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
+    const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
+    kfn<<<grid, threads, smem, st>>>(tin, tout, p);
+    return cuda_status(cudaGetLastError());
+  }
+}
+
+template <class P, bool WIDE>
+int launch_tmem_policy(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, int block, int items,
+                       cudaStream_t st) {
+  if (block == 128 && items == 32) return launch_tmem_shape<P, 128, 32, WIDE>(p, tin, tout, st);
+  if (block == 256 && items == 16) return launch_tmem_shape<P, 256, 16, WIDE>(p, tin, tout, st);
+  if (block == 256 && items == 32) return launch_tmem_shape<P, 256, 32, WIDE>(p, tin, tout, st);
+  return B2P_ERR_UNSUPPORTED;
+}
+
+// Shared-memory layout of the TMEM-staged kernel for (block, items): input
+// stages, two output stages, thread prefixes of every slot; as many slots as
+// 512 TMEM columns hold.  False when the policy or shape has no TMEM kernel.
+template <class P>
+bool tmem_layout(TmaParams &p, int block, int items) {
+  constexpr size_t es = sizeof(typename P::In), eo = sizeof(typename P::Out);
+  if (!kUseTmem || !TmemExact<P>::value || (block != 128 && block != 256)) return false;
+  const int cols = items * (int)eo / 4;
+  if (cols != 16 && cols != 32) return false;
+  const int slots = std::min(kMaxStages, 512 / (cols * block / 128));
+  const size_t in_b = (size_t)block * items * es, out_b = (size_t)block * items * eo;
+  const size_t texcl = ((size_t)slots * block * sizeof(typename P::Acc) + 1023) & ~size_t(1023);
+  const int so = 2;
+  if (so * out_b + texcl + 2 * in_b > kSmemBudget) return false;
+  const int si = (int)std::min<size_t>(kMaxStages, (kSmemBudget - so * out_b - texcl) / in_b);
+  p.stages = si;
+  p.stage_stride = (unsigned)in_b;
+  p.slots = slots;
+  p.out_stages = so;
+  p.out_stage_stride = (unsigned)out_b;
+  p.out_base = (unsigned)(si * in_b);
+  p.texcl_base = (unsigned)(si * in_b + so * out_b);
+  return true;
+}
+
 template <class P, bool WIDE>
 int launch_policy(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, int block, int items,
                   cudaStream_t st) {
@@ -767,7 +1153,6 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
   const size_t in_bytes = (size_t)tile * es;
   const size_t stage = in_bytes + (eo != es ? (size_t)tile * eo : 0);
   const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stage + block * sizeof(typename P::Acc)));
-  if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
   p.ntiles = (long long)((n + tile - 1) / tile);
@@ -795,6 +1180,13 @@ int launch_t(int inclusive, const void *in, void *out, size_t n, const void *ini
       !encode_row_tensor(&tout, out, (unsigned long long)p.rows_full_out,
                          (int)std::min<long long>(256, tile / epr_out)))
     return B2P_ERR_UNSUPPORTED;
+  if (tmem_layout<P>(p, block, items)) {
+    if constexpr (P::kCompensated) {
+      if (wide) return launch_tmem_policy<P, true>(p, tin, tout, block, items, st);
+    }
+    return launch_tmem_policy<P, false>(p, tin, tout, block, items, st);
+  }
+  if (stages < kMinStages) return B2P_ERR_UNSUPPORTED;
   if constexpr (P::kCompensated) {
     if (wide) return launch_policy<P, true>(p, tin, tout, block, items, st);
   }
@@ -915,7 +1307,7 @@ bool scan_tma_shape(int dtype, int block, int items) {
   const size_t es = dtype_size(dtype), eo = acc_size(dtype);
   const size_t stage = (size_t)block * items * (es + (eo != es ? eo : 0));
   const size_t acc = dtype_is_float(dtype) && dtype != B2P_F64 ? 8 : acc_size(dtype);
-  return shape && (stage + (size_t)block * acc) * 3 <= kSmemBudget;
+  return shape && (stage + (size_t)block * acc) * kMinStages <= kSmemBudget;
 }
 
 int launch_scan_tma(int dtype, int op, int inclusive, const void *in, void *out, size_t n, const void *init,
@@ -941,7 +1333,7 @@ bool copy_if_tma_shape(int dtype, int block, int items) {
   const size_t es = dtype_size(dtype);
   if (es != 4 && es != 8) return false;
   const bool shape = (block == 128 && items == 32) || (block == 256 && items == 16) || (block == 256 && items == 32);
-  return shape && ((size_t)block * items * es + 1024 + (size_t)block * 12) * 3 <= kSmemBudget;
+  return shape && ((size_t)block * items * es + 1024 + (size_t)block * 12) * kMinStages <= kSmemBudget;
 }
 
 int launch_copy_if_tma(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs,
