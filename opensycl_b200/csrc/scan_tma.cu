@@ -51,6 +51,8 @@ constexpr size_t kSmemBudget = 210 * 1024;  // stages + thread prefixes
 // Scans stage tiles that wait for their carries in TMEM where the policy
 // and shape allow it.
 constexpr bool kUseTmem = true;
+// Output stages of the TMEM-staged copy_if.
+constexpr int kCopyOutStages = 2;
 
 // Threads of a pipelined block with NC reducer and NC emitter threads.
 constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
@@ -99,6 +101,7 @@ struct PipeState {
   // back by the store warp, tile ids of input and output stages, TMEM base
   uint64_t slot_free[kMaxStages], out_empty[kMaxStages];
   long long tile_in[kMaxStages], tile_out[kMaxStages];
+  unsigned long long out_carry[kMaxStages], out_count[kMaxStages];  // copy_if: output stage's position, count
   uint32_t tmem_base;
   unsigned long long agg[kMaxStages], carry[kMaxStages];
   unsigned long long epoch;
@@ -1046,6 +1049,256 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   finish_launch(p.hdr, epoch, nullptr, 0);
 }
 
+// -------------------------------------------------- copy_if, TMEM-staged
+//
+// copy_if_tma_kernel's compaction with the TMEM staging of scan_tmem_kernel:
+// reducers park each thread's raw elements in a TMEM slot (keep masks and
+// thread offsets beside it in shared memory) and hand the input stage back
+// at once; emitters pack the kept elements into an output stage.
+//
+// Thread t owns elements t * ITEMS .. t * ITEMS + ITEMS - 1 (16-byte reads
+// of the swizzled stage) and packs them in order.  Both groups work through
+// one tile at a time, so the per-element work is kept to a few instructions;
+// the price is bank conflicts in the packing stores for regular keep patterns
+// (every lane keeping 32 elements puts all 32 lanes of a store on one bank),
+// where the pipeline falls to about 1.8 TB/s.  A warp-striped layout with
+// ballot packing, and lane-rotated element order, were both measured: free
+// of conflicts, but slower at typical selectivities.
+
+// Keep bits of a thread's ITEMS elements (w: the elements as 32-bit words,
+// element j at tile index first + j); only the first `count` elements of the
+// tile are real.
+template <class T, int ITEMS, int CMP>
+__device__ __forceinline__ unsigned keep_bits(const uint32_t *w, unsigned long long mask64,
+                                              unsigned long long rhs64, int first, int count) {
+  using U = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
+  const U mask = (U)mask64, rhs = (U)rhs64;
+  unsigned keep = 0;
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    U e;
+    memcpy(&e, w + j * (int)(sizeof(T) / 4), sizeof(T));
+    const U a = e & mask;
+    bool kb;
+    if constexpr (CMP == B2P_CMP_LT) kb = a < rhs;
+    else if constexpr (CMP == B2P_CMP_LE) kb = a <= rhs;
+    else if constexpr (CMP == B2P_CMP_EQ) kb = a == rhs;
+    else if constexpr (CMP == B2P_CMP_NE) kb = a != rhs;
+    else if constexpr (CMP == B2P_CMP_GE) kb = a >= rhs;
+    else kb = a > rhs;
+    keep |= (unsigned)kb << j;
+  }
+  if (count < first + ITEMS) keep &= count <= first ? 0u : ((1u << (count - first)) - 1u);  // count - first < 32 here
+  return keep;
+}
+
+template <class T, int NC, int ITEMS, int CMP>
+__global__ void __launch_bounds__(pipe_threads(NC), 1)
+    copy_if_tmem_kernel(const __grid_constant__ CUtensorMap tin, TmaParams p) {
+  constexpr int kTile = NC * ITEMS;
+  constexpr int kEpr = 128 / (int)sizeof(T);
+  static_assert(kTile % (8 * kEpr) == 0, "a stage is a whole number of 1024-byte swizzle atoms");
+  constexpr int kRows = kTile / kEpr;
+  constexpr int kBox = kRows < 256 ? kRows : 256;
+  static_assert(kRows % kBox == 0, "box rows");
+  static_assert(ITEMS <= 32, "keep mask is 32 bits");
+  static_assert(kTile <= 65536, "thread offsets are 16 bits");
+  constexpr int kCols = ITEMS * (int)sizeof(T) / 4;
+  static_assert(kCols == 16 || kCols == 32, "TMEM columns per thread");
+  static_assert(NC % 128 == 0, "reducer and emitter groups cover the four TMEM lane quarters evenly");
+  constexpr int kSlotCols = kCols * (NC / 128);
+
+  extern __shared__ char smem_raw[];
+  char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  char *obase = smem + p.out_base;
+  unsigned *keep_all = reinterpret_cast<unsigned *>(smem + p.texcl_base);
+  uint16_t *texcl_all = reinterpret_cast<uint16_t *>(keep_all + (size_t)p.slots * NC);  // offsets < 2^16
+  __shared__ __align__(8) PipeState ps;
+  __shared__ unsigned long long s_warp[32];
+  __shared__ int s_go[2];
+
+  const int warp = threadIdx.x >> 5;
+  tmem_pipe_init(ps, p, NC / 32);
+  if (warp == 0) {
+    __syncwarp();
+    tmem_alloc(&ps.tmem_base, 512);
+  }
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tbase = ps.tmem_base;
+  const unsigned long long epoch = ps.epoch;
+  const unsigned long long epoch_tag = epoch << 8;
+  const int SI = p.stages, SL = p.slots, SO = p.out_stages;
+  const long long last = p.ntiles - 1;
+  const int ntail = (int)(p.n - p.tail_begin);
+  T *out = reinterpret_cast<T *>(p.out);
+
+  if (warp < NC / 32) {
+    // ------------------------------------------------------------ reducers
+    const int t = threadIdx.x;
+    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * kCols);
+    long long it = 0;
+    RingPos ri, rs;
+    for (;; ++it, ri.advance(1, SI), rs.advance(1, SL)) {
+      if (t == 0) {
+        int go = mbar_wait(&ps.full[ri.s], ri.ph, p.timeout_ns) ? 1 : -1;
+        if (go > 0 && ps.tile_in[ri.s] < 0) go = 0;
+        if (go > 0 && !mbar_wait(&ps.slot_free[rs.s], rs.ph ^ 1u, p.timeout_ns)) go = -1;
+        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        s_go[0] = go;
+      }
+      bar_named(1, NC);
+      if (s_go[0] <= 0) break;
+      (void)mbar_try(&ps.full[ri.s], ri.ph);  // completed: this thread's acquire of the TMA bytes
+      tmem_fence_after();
+      const long long tile = ps.tile_in[ri.s];
+      char *buf = smem + (size_t)ri.s * p.stage_stride;
+      if (tile == last && ntail > 0) load_row_tail<T, NC>(p, buf, tile, kTile);
+      uint32_t w[kCols];
+#pragma unroll
+      for (int k = 0; k < kCols / 4; ++k) {
+        const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * (kCols / 4) + k) * 16);
+        w[4 * k] = u.x;
+        w[4 * k + 1] = u.y;
+        w[4 * k + 2] = u.z;
+        w[4 * k + 3] = u.w;
+      }
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.empty[ri.s]);  // this warp is done with the input stage
+      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
+      tmem_st16(ta, w);
+      if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
+      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
+      const unsigned keep = keep_bits<T, ITEMS, CMP>(w, p.mask, p.rhs, t * ITEMS, count);
+      unsigned long long tile_kept;
+      const unsigned long long ex =
+          group_exclusive_scan<CountOps, NC>((unsigned long long)__popc(keep), s_warp, &tile_kept, t, 1);
+      texcl_all[(size_t)rs.s * NC + t] = (uint16_t)ex;
+      keep_all[(size_t)rs.s * NC + t] = keep;
+      tmem_wait_st();
+      tmem_fence_before();
+      bar_named(1, NC);  // slot, keep masks and offsets complete
+      if (t == 0) {
+        if (tile != p.stall_tile)
+          st_status(p.status + tile, tile_kept, epoch_tag | (tile == 0 ? kFlagPrefix : kFlagAgg));
+        ps.tile[rs.s] = tile;
+        ps.agg[rs.s] = tile_kept;
+        mbar_arrive(&ps.aggr[rs.s]);
+      }
+    }
+    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
+  } else if (warp < 2 * NC / 32) {
+    // ------------------------------------------------------------ emitters
+    const int t = threadIdx.x - NC;
+    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(((t >> 5) >> 2) * kCols);
+    RingPos rs, ro;
+    for (long long it = 0;; ++it, rs.advance(1, SL), ro.advance(1, SO)) {
+      if (t == 0) {
+        int go = emitter_wait(p, ps, rs, it);
+        if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
+        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        if (go == 0) {
+          mbar_arrive(&ps.emitted[ro.s]);
+          RingPos r = rs;
+          for (int j = 0; j < kLookWarps; ++j, r.advance(1, SL)) mbar_arrive(&ps.aggr[r.s]);
+        }
+        s_go[1] = go;
+      }
+      bar_named(2, NC);
+      if (s_go[1] <= 0) break;
+      tmem_fence_after();
+      const long long tile = ps.tile[rs.s];
+      const unsigned long long carry = ps.carry[rs.s];
+      unsigned long long kept_total = ps.agg[rs.s];
+      if (carry > p.n || kept_total > p.n - carry) {  // only after a broken chain: write nothing
+        if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        kept_total = 0;
+      }
+      const unsigned keep = keep_all[(size_t)rs.s * NC + t];
+      const unsigned o = texcl_all[(size_t)rs.s * NC + t];
+      uint32_t w[kCols];
+      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
+      if constexpr (kCols == 32) tmem_load32(ta, w);
+      else tmem_load16(ta, w);
+      tmem_fence_before();
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.slot_free[rs.s]);  // slot, masks and offsets read
+      char *obuf = obase + (size_t)ro.s * p.out_stage_stride;
+      const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
+      const unsigned phase = (unsigned)(g0 & 15u);
+      const unsigned lim = (unsigned)kept_total;
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) {
+        const unsigned pos = o + __popc(keep & ((1u << j) - 1u));
+        if (((keep >> j) & 1u) && pos < lim) {
+          T v;
+          memcpy(&v, w + j * (int)(sizeof(T) / 4), sizeof(T));
+          *reinterpret_cast<T *>(obuf + phase + pos * sizeof(T)) = v;  // phase is a multiple of sizeof(T)
+        }
+      }
+      fence_async_smem();
+      bar_named(2, NC);
+      const uintptr_t g1 = g0 + kept_total * sizeof(T);
+      const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
+      const bool mid = a1 > a0;
+      const long long nhead = mid ? (long long)((a0 - g0) / sizeof(T)) : (long long)kept_total;
+      const long long tail0 = mid ? (long long)((a1 - g0) / sizeof(T)) : (long long)kept_total;
+      const long long ntl = (long long)kept_total - tail0;
+      if (t < nhead) out[carry + t] = *reinterpret_cast<const T *>(obuf + phase + t * sizeof(T));
+      if (t >= 32 && t - 32 < ntl) {
+        const long long k = tail0 + (t - 32);
+        out[carry + k] = *reinterpret_cast<const T *>(obuf + phase + k * sizeof(T));
+      }
+      if (t == 0 && tile == last && p.num_copied) *p.num_copied = carry + kept_total;
+      bar_named(2, NC);  // the plain stores are done with the output stage
+      if (t == 0) {
+        ps.out_carry[ro.s] = carry;
+        ps.out_count[ro.s] = kept_total;
+        mbar_arrive(&ps.emitted[ro.s]);
+      }
+    }
+  } else if (warp < 2 * NC / 32 + kLookWarps) {
+    lookback_loop<CountOps>(p, ps, warp - 2 * NC / 32, 0ull, epoch_tag, SL);
+  } else if (warp == 2 * NC / 32 + kLookWarps) {
+    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile_in);
+  } else {
+    // ---------------------------------------------------------- store warp
+    if ((threadIdx.x & 31) == 0) {
+      RingPos ro;
+      for (long long it = 0;; ++it, ro.advance(1, SO)) {
+        if (!mbar_wait(&ps.emitted[ro.s], ro.ph, p.timeout_ns)) {
+          record_error(p.hdr, B2P_ERR_TIMEOUT);
+          break;
+        }
+        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+        const unsigned long long carry = ps.out_carry[ro.s];
+        const unsigned long long kept_total = ps.out_count[ro.s];
+        const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
+        const uintptr_t g1 = g0 + kept_total * sizeof(T);
+        const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
+        if (a1 > a0) {
+          const char *src = obase + (size_t)ro.s * p.out_stage_stride + (g0 & 15u) + (a0 - g0);
+          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(a0),
+                       "r"(smem_u32(src)), "r"((unsigned)(a1 - a0))
+                       : "memory");
+        }
+        bulk_commit();
+        bulk_wait_read<0>();
+        mbar_arrive(&ps.out_empty[ro.s]);
+      }
+      bulk_wait_all();
+    }
+  }
+  tmem_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(tbase, 512);
+  }
+  finish_launch(p.hdr, epoch, nullptr, 0);
+}
+
 // ------------------------------------------------------------------ host
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -1232,8 +1485,36 @@ int launch_copy_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
+template <class T, int NC, int ITEMS, int CMP>
+int launch_copy_tmem_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
+  constexpr int cols = ITEMS * (int)sizeof(T) / 4;
+  if constexpr (cols != 16 && cols != 32) {
+    return B2P_ERR_UNSUPPORTED;
+  } else {
+    auto kfn = copy_if_tmem_kernel<T, NC, ITEMS, CMP>;
+    const size_t smem = p.texcl_base + (size_t)p.slots * NC * 6 + 1024;
+    int rc = ensure_dynamic_smem((const void *)kfn, smem);
+    if (rc) return rc;
+    const int threads = pipe_threads(NC);
+    if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
+    const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
+    kfn<<<grid, threads, smem, st>>>(tin, p);
+    return cuda_status(cudaGetLastError());
+  }
+}
+
 template <class T, int NC, int ITEMS>
 int launch_copy_items(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
+  if (p.slots > 0) {
+    switch (p.cmp) {
+    case B2P_CMP_LT: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_LT>(p, tin, st);
+    case B2P_CMP_LE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_LE>(p, tin, st);
+    case B2P_CMP_EQ: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_EQ>(p, tin, st);
+    case B2P_CMP_NE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_NE>(p, tin, st);
+    case B2P_CMP_GE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_GE>(p, tin, st);
+    default: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_GT>(p, tin, st);
+    }
+  }
   switch (p.cmp) {
   case B2P_CMP_LT: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_LT>(p, tin, st);
   case B2P_CMP_LE: return launch_copy_shape<T, NC, ITEMS, B2P_CMP_LE>(p, tin, st);
@@ -1252,6 +1533,31 @@ int launch_copy_cmp(TmaParams &p, const CUtensorMap &tin, int block, int items, 
   return B2P_ERR_UNSUPPORTED;
 }
 
+// Shared-memory layout of the TMEM-staged copy_if for (block, items):
+// input stages, two output stages (a tile plus 1024 bytes for the output's
+// 16-byte phase), thread offsets and keep masks of every slot.  Leaves
+// p.slots = 0 (in-place kernel) when the shape has no TMEM kernel.
+bool copy_tmem_layout(TmaParams &p, size_t es, int block, int items) {
+  p.slots = 0;
+  if (!kUseTmem || (block != 128 && block != 256)) return false;
+  const int cols = items * (int)es / 4;
+  if (cols != 16 && cols != 32) return false;
+  const int slots = std::min(kMaxStages, 512 / (cols * block / 128));
+  const size_t in_b = (size_t)block * items * es, out_b = in_b + 1024;
+  const size_t side = ((size_t)slots * block * 6 + 1023) & ~size_t(1023);
+  const int so = kCopyOutStages;
+  if (so * out_b + side + 2 * in_b > kSmemBudget) return false;
+  const int si = (int)std::min<size_t>(kMaxStages, (kSmemBudget - so * out_b - side) / in_b);
+  p.stages = si;
+  p.stage_stride = (unsigned)in_b;
+  p.slots = slots;
+  p.out_stages = so;
+  p.out_stage_stride = (unsigned)out_b;
+  p.out_base = (unsigned)(si * in_b);
+  p.texcl_base = (unsigned)(si * in_b + so * out_b);
+  return true;
+}
+
 template <class T>
 int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, uint64_t rhs, uint64_t *num_copied,
                   void *scratch, int block, int items, cudaStream_t st) {
@@ -1259,7 +1565,6 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   const long long tile = (long long)block * items;
   const size_t stride = (size_t)tile * es + 1024;
   const int stages = (int)std::min<size_t>(kMaxStages, kSmemBudget / (stride + block * (sizeof(unsigned long long) + 4)));
-  if (stages < 3) return B2P_ERR_UNSUPPORTED;
   TmaParams p{};
   p.n = n;
   p.ntiles = (long long)((n + tile - 1) / tile);
@@ -1279,6 +1584,7 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
   p.rhs = rhs;
   p.cmp = cmp;
   p.num_copied = reinterpret_cast<unsigned long long *>(num_copied);
+  if (!copy_tmem_layout(p, es, block, items) && stages < kMinStages) return B2P_ERR_UNSUPPORTED;
   CUtensorMap tin;
   if (!encode_row_tensor(&tin, in, (unsigned long long)p.rows_full, (int)std::min<long long>(256, tile / epr)))
     return B2P_ERR_UNSUPPORTED;

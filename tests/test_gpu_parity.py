@@ -366,6 +366,34 @@ def test_copy_if_pipelined_unaligned_output(dev, code):
                 assert np.array_equal(to_np(out[:k]), ref), (cfg, n, shift)
 
 
+@pytest.mark.parametrize("code", [C.U32, C.U64])
+def test_copy_if_pipelined_regular_patterns(dev, code):
+    """Regular keep patterns through the pipelined copy_if kernels: all kept
+    (the output is the input), none kept, every other element, one element
+    per tile; sizes with a partial last tile."""
+    rng = np.random.default_rng(870 + code)
+    for cfg in TMA_SCAN_CONFIGS:
+        blk, items = C.config_describe(cfg)[:2]
+        tile = blk * items
+        n = 5 * tile + 77
+        u = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(NP[code])
+        u = (u & ~np.array(7, dtype=NP[code])) | (np.arange(n) % 8).astype(NP[code])  # low 3 bits = index mod 8
+        xd = to_dev(u, code)
+        for cmp, rhs in [(C.CMP_LT, 8), (C.CMP_GT, 7), (C.CMP_EQ, 0), (C.CMP_LT, 4)]:
+            keep = (u & 7) < 8 if (cmp, rhs) == (C.CMP_LT, 8) else \
+                (u & 7) > 7 if cmp == C.CMP_GT else (u & 7) == 0 if cmp == C.CMP_EQ else (u & 7) < 4
+            ref = u[keep]
+            out, cnt = C.copy_if(xd, 7, cmp, rhs, config=cfg)
+            k = int(cnt.item())
+            assert k == ref.size, (cfg, cmp, rhs)
+            assert np.array_equal(to_np(out[:k]), ref), (cfg, cmp, rhs)
+        # one kept element per tile
+        v = np.zeros(n, dtype=NP[code])
+        v[::tile] = 1
+        out, cnt = C.copy_if(to_dev(v, code), 1, C.CMP_EQ, 1, config=cfg)
+        assert int(cnt.item()) == v[::tile].size and np.all(to_np(out[:int(cnt.item())]) == 1)
+
+
 def test_copy_if_oracle_u32(dev):
     rng = np.random.default_rng(11)
     x = rng.integers(0, 1 << 32, 1 << 20, dtype=np.uint64).astype(np.uint32)
