@@ -53,6 +53,11 @@ constexpr size_t kSmemBudget = 210 * 1024;  // stages + thread prefixes
 constexpr bool kUseTmem = true;
 // Output stages of the TMEM-staged copy_if.
 constexpr int kCopyOutStages = 2;
+// Output stages of the TMEM-staged scan, and the bulk tensor stores its
+// store warp keeps in flight (at most kScanOutStages - 1).
+constexpr int kScanOutStages = 2;
+constexpr int kTmemStoresInFlight = 1;
+constexpr int kScanMaxInStages = kMaxStages;
 
 // Threads of a pipelined block with NC reducer and NC emitter threads.
 constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
@@ -400,19 +405,21 @@ __device__ __forceinline__ void emitters_finish(const TmaParams &p, PipeState &p
 // Store warp: stages whose bulk stores were committed but may still read
 // shared memory.  A stage is handed back to the producer (empty barrier)
 // once its store has read it; up to kStoresInFlight stores overlap.
+template <int D = kStoresInFlight>
 struct StoreRelease {
   RingPos oldest;
   int pending = 0;
-  __device__ __forceinline__ void committed(PipeState &ps, int S) {
-    if (++pending < kStoresInFlight) return;
-    bulk_wait_read<kStoresInFlight - 1>();
-    mbar_arrive(&ps.empty[oldest.s]);
+  // after committing a store group for the ring of S barriers `freed`
+  __device__ __forceinline__ void committed(uint64_t *freed, int S) {
+    if (++pending < D) return;
+    bulk_wait_read<D - 1>();
+    mbar_arrive(&freed[oldest.s]);
     oldest.advance(1, S);
     --pending;
   }
-  __device__ __forceinline__ void drain(PipeState &ps, int S) {
+  __device__ __forceinline__ void drain(uint64_t *freed, int S) {
     bulk_wait_read<0>();
-    for (; pending > 0; --pending, oldest.advance(1, S)) mbar_arrive(&ps.empty[oldest.s]);
+    for (; pending > 0; --pending, oldest.advance(1, S)) mbar_arrive(&freed[oldest.s]);
   }
 };
 
@@ -543,7 +550,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       prefetch_tensormap(&tout);
       const unsigned long long spol = l2_policy_stream();
       RingPos r;
-      StoreRelease rel;
+      StoreRelease<> rel;
       for (long long it = 0;; ++it, r.advance(1, S)) {
         const int s = r.s;
         if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
@@ -557,9 +564,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         for (long long rr = 0; rr < rows_out; rr += kBoxOut)
           tma_store_2d(&tout, 0, (int)(r0 + rr), smem + (size_t)s * p.stage_stride + p.out_offset + rr * 128, spol);
         bulk_commit();
-        rel.committed(ps, S);
+        rel.committed(ps.empty, S);
       }
-      rel.drain(ps, S);
+      rel.drain(ps.empty, S);
       bulk_wait_all();
     }
   }
@@ -830,6 +837,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       prefetch_tensormap(&tout);
       const unsigned long long spol = l2_policy_stream();
       RingPos ro;
+      StoreRelease<kTmemStoresInFlight> rel;
       for (long long it = 0;; ++it, ro.advance(1, SO)) {
         if (!mbar_wait(&ps.emitted[ro.s], ro.ph, p.timeout_ns)) {
           record_error(p.hdr, B2P_ERR_TIMEOUT);
@@ -842,9 +850,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         const char *src = obase + (size_t)ro.s * p.out_stage_stride;
         for (long long rr = 0; rr < rows_out; rr += kBoxOut) tma_store_2d(&tout, 0, (int)(r0 + rr), src + rr * 128, spol);
         bulk_commit();
-        bulk_wait_read<0>();
-        mbar_arrive(&ps.out_empty[ro.s]);
+        rel.committed(ps.out_empty, SO);
       }
+      rel.drain(ps.out_empty, SO);
       bulk_wait_all();
     }
   }
@@ -1019,7 +1027,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
     // ---------------------------------------------------------- store warp
     if ((threadIdx.x & 31) == 0) {
       RingPos r;
-      StoreRelease rel;
+      StoreRelease<> rel;
       for (long long it = 0;; ++it, r.advance(1, S)) {
         const int s = r.s;
         if (!mbar_wait(&ps.emitted[s], r.ph, p.timeout_ns)) {
@@ -1040,9 +1048,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
                        : "memory");
         }
         bulk_commit();
-        rel.committed(ps, S);
+        rel.committed(ps.empty, S);
       }
-      rel.drain(ps, S);
+      rel.drain(ps.empty, S);
       bulk_wait_all();
     }
   }
@@ -1372,9 +1380,9 @@ bool tmem_layout(TmaParams &p, int block, int items) {
   const int slots = std::min(kMaxStages, 512 / (cols * block / 128));
   const size_t in_b = (size_t)block * items * es, out_b = (size_t)block * items * eo;
   const size_t texcl = ((size_t)slots * block * sizeof(typename P::Acc) + 1023) & ~size_t(1023);
-  const int so = 2;
+  const int so = kScanOutStages;
   if (so * out_b + texcl + 2 * in_b > kSmemBudget) return false;
-  const int si = (int)std::min<size_t>(kMaxStages, (kSmemBudget - so * out_b - texcl) / in_b);
+  const int si = (int)std::min<size_t>(kScanMaxInStages, (kSmemBudget - so * out_b - texcl) / in_b);
   p.stages = si;
   p.stage_stride = (unsigned)in_b;
   p.slots = slots;
