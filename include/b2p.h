@@ -242,9 +242,11 @@ int b2p_segmented_per_call(int prim, int dtype, int op, const void *in, void *ou
                            size_t scratch_bytes, int config, b2p_stream stream);
 
 /* Wait for `stream`, then read the sticky device error word kept in
- * `scratch` (B2P_OK or B2P_ERR_TIMEOUT); clear != 0 resets it.  Blocks the
- * host.  Stands in for the reference's asynchronous error list
- * (runtime/error.hpp) that event::wait() rethrows. */
+ * `scratch` (B2P_OK or B2P_ERR_TIMEOUT); clear != 0 resets it.  scratch ==
+ * NULL reads the library's own word for the calls that take no scratch
+ * (b2p_histogram_u8) on the current device.  Blocks the host.  Stands in
+ * for the reference's asynchronous error list (runtime/error.hpp) that
+ * event::wait() rethrows. */
 int b2p_device_error(void *scratch, b2p_stream stream, int clear);
 
 /* Process-wide bound for every device-side wait, in nanoseconds

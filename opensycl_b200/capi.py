@@ -321,10 +321,13 @@ def segmented_scan(x, offsets, inclusive=True, op="sum", init=None, out=None, co
     return out
 
 
-def device_error(stream=None, clear=True) -> int:
-    """Sticky device-side error recorded in this stream's scratch."""
+def device_error(stream=None, clear=True, scratchless=False) -> int:
+    """Sticky device-side error recorded in this stream's scratch, or with
+    scratchless=True the library's word for calls without scratch (histogram)."""
     torch = _torch()
     s = stream if stream is not None else torch.cuda.current_stream()
+    if scratchless:
+        return lib().b2p_device_error(None, _stream(s), int(clear))
     buf = Scratch.get(256, s)
     return lib().b2p_device_error(ctypes.c_void_p(_aligned_ptr(buf)), _stream(s), int(clear))
 

@@ -353,9 +353,9 @@ int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in, void *o
 }
 
 int b2p_device_error(void *scratch, b2p_stream stream, int clear) {
-  if (!scratch) return B2P_ERR_SCRATCH;
   cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_status(e);
+  if (!scratch) return scratchless_error(clear);
   unsigned v = 0;
   ScratchHeader *h = reinterpret_cast<ScratchHeader *>(scratch);
   e = cudaMemcpy(&v, &h->error, sizeof(v), cudaMemcpyDefault);

@@ -71,6 +71,10 @@ int launch_copy_if_tma(int dtype, const void *in, void *out, size_t n, uint64_t 
 bool copy_if_config_valid(int dtype, int config);
 
 // Histogram.
+// The device error word of scratch-less calls (histogram); clear != 0
+// resets it.  Synchronous.
+int scratchless_error(int clear);
+
 int launch_histogram_u8(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,
                         cudaStream_t s);
 

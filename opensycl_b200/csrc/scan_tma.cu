@@ -113,19 +113,6 @@ struct PipeState {
   long long end_item;  // number of tiles this block handles, once the reducers know it
 };
 
-// Position in the ring of stages: stage index and mbarrier phase parity of
-// an item, advanced without divisions.
-struct RingPos {
-  int s = 0;
-  unsigned ph = 0;
-  __device__ __forceinline__ void advance(int k, int S) {
-    s += k;
-    while (s >= S) {
-      s -= S;
-      ph ^= 1u;
-    }
-  }
-};
 
 // --------------------------------------------------- per-thread tile passes
 // `t` is the thread's index inside its warp group (reducers or emitters).

@@ -118,6 +118,20 @@ __device__ __forceinline__ void bar_named(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// Position in the ring of stages: stage index and mbarrier phase parity of
+// an item, advanced without divisions.
+struct RingPos {
+  int s = 0;
+  unsigned ph = 0;
+  __device__ __forceinline__ void advance(int k, int S) {
+    s += k;
+    while (s >= S) {
+      s -= S;
+      ph ^= 1u;
+    }
+  }
+};
+
 // Host: describe [base, base + rows * 128) as a tensor of `rows` rows of 128
 // bytes, read and written in boxes of box_rows rows with the 128-byte
 // swizzle.  base must be 16-byte aligned, 1 <= rows < 2^31, 1 <= box_rows

@@ -425,6 +425,24 @@ def test_histogram_bit_exact(dev):
                         assert np.array_equal(bins.cpu().numpy().astype(np.int64), ref), (n, dist, nbins, off, cfg)
 
 
+def test_histogram_streamed_chunks(dev):
+    """Grid mode 1 streams keys through a ring of shared stages with bulk
+    copies: many chunks per block (the ring wraps), a partial last chunk,
+    unaligned heads and ragged tails; the scratch-less error word stays clear."""
+    rng = np.random.default_rng(13)
+    for n in [(40 << 20) + 3, (9 << 20) + 4095]:
+        k = C.synth_fill(4, int(rng.integers(1 << 30)), n, 1.2)
+        ref = O.histogram_u8(k, 256).astype(np.int64)
+        for off in (0, 1, 15):
+            for cfg in (23, 30, 31):
+                assert C.config_describe(cfg)[2] == 1
+                bins = torch.zeros(256, dtype=torch.int32, device="cuda")
+                kd = torch.from_numpy(np.concatenate([np.zeros(off, np.uint8), k])).cuda()[off:]
+                C.histogram_u8(kd, bins=bins, config=cfg)
+                assert np.array_equal(bins.cpu().numpy().astype(np.int64), ref), (n, off, cfg)
+    assert C.device_error(scratchless=True) == C.OK
+
+
 # ------------------------------------------------------------------ errors
 
 def test_errors_are_status_codes(dev):
