@@ -236,7 +236,7 @@ def main():
     scan_cfg = C.lib().b2p_auto_config(C.PRIM_SCAN, C.F32, n, 0, 0.0)
     dot_cfg = C.lib().b2p_auto_config(C.PRIM_DOT, C.F32, n, 0, 0.0)
     scan_blk, scan_items, scan_mode = C.config_describe(scan_cfg)
-    scan_name = (f"scan_tma_kernel<f32 sum,{scan_blk}x{scan_items}>" if scan_mode == 1
+    scan_name = (f"scan_tmem_kernel<f32 sum,{scan_blk}x{scan_items}>" if scan_mode == 1
                  else f"scan_{'lookback' if scan_mode == 0 else 'twophase'}_kernel<f32 sum,{scan_blk}x{scan_items}>")
     kern = {scan_name: (scan_ms, 8.0 * n), "reduce_kernel<f32 dot>": (dot_ms, 8.0 * n)}
     dom = max(kern, key=lambda k: kern[k][0])

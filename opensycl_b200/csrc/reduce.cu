@@ -108,8 +108,15 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
   const int B = min(p.B, kMaxB);
   const unsigned long long epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
 
+  // Compensated folds keep kChains accumulators (element e of each vector
+  // goes to chain e % kChains: two for fp32, four for bf16), shortening the
+  // dependent TwoSum chain; the order depends only on element positions, so
+  // every launch configuration gives the same bits.
+  constexpr int kChains = !P::kCompensated || V == 1 ? 1 : (V >= 8 ? 4 : 2);
   for (long long run = gw; run < p.runs; run += tw) {
-    Acc acc = P::identity();
+    Acc acc[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) acc[c] = P::identity();
     const long long base = run * 32LL * p.K + lane;
     for (int j0 = 0; j0 < p.K; j0 += B) {
       const long long v0 = base + (long long)j0 * 32;
@@ -129,7 +136,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
             for (int e = 0; e < V; ++e) {
               In xa = vec_elem<In>(va[k], e);
               In xb = DOT ? vec_elem<In>(vb[k], e) : xa;
-              fold<P, DOT>(acc, xa, xb);
+              fold<P, DOT>(acc[e % kChains], xa, xb);
             }
           }
       } else {
@@ -142,14 +149,20 @@ __global__ void __launch_bounds__(1024) reduce_kernel(ReduceParams p) {
             if constexpr (DOT) xb = load_vec<In, VEC>(b, vi);
 #pragma unroll
             for (int e = 0; e < V; ++e)
-              fold<P, DOT>(acc, vec_elem<In>(xa, e), DOT ? vec_elem<In>(xb, e) : vec_elem<In>(xa, e));
+              fold<P, DOT>(acc[e % kChains], vec_elem<In>(xa, e), DOT ? vec_elem<In>(xb, e) : vec_elem<In>(xa, e));
           }
         }
       }
     }
-    if constexpr (P::kCompensated) acc = df_norm(acc);
-    acc = warp_allreduce<P>(acc);
-    if (lane == 0) st_status(p.partials + run, P::pack(acc), (epoch << 8) | kFlagAgg);
+    if constexpr (kChains == 4) {
+      acc[0] = P::combine(acc[0], acc[1]);
+      acc[2] = P::combine(acc[2], acc[3]);
+    }
+    if constexpr (kChains >= 2) acc[0] = P::combine(acc[0], acc[kChains / 2]);
+    Acc r = acc[0];
+    if constexpr (P::kCompensated) r = df_norm(r);
+    r = warp_allreduce<P>(r);
+    if (lane == 0) st_status(p.partials + run, P::pack(r), (epoch << 8) | kFlagAgg);
   }
 
   // ---- last block to arrive combines everything (no waiting).
