@@ -1,8 +1,9 @@
 // Offloaded C++ standard parallel algorithms on the primitive path:
 // std::reduce (3 overloads), std::transform_reduce (3), std::inclusive_scan
-// (3), std::exclusive_scan (2) and std::copy_if, taking the execution policy
-// b2p_stdpar::par_unseq (AdaptiveCpp: the par_unseq overloads of
-// std/stdpar/pstl-impl/numeric.hpp:28-467 and pstl-impl/algorithm.hpp:150-187,
+// (3), std::exclusive_scan (2), std::transform_inclusive_scan (2),
+// std::transform_exclusive_scan (1) and std::copy_if, taking the execution
+// policy b2p_stdpar::par_unseq (AdaptiveCpp: the par_unseq overloads of
+// std/stdpar/pstl-impl/numeric.hpp:28-576 and pstl-impl/algorithm.hpp:150-187,
 // which its compiler pass substitutes for std::execution::par_unseq; here
 // the caller names the policy).
 //
@@ -244,6 +245,40 @@ template <class InputIt, class OutputIt, class T>
 OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &p, InputIt first, InputIt last, OutputIt d_first,
                         T init) {
   return std::exclusive_scan(p, first, last, d_first, init, std::plus<>{});
+}
+
+// ------------------------------------------------------- transform scans
+// (pstl-impl/numeric.hpp:469-576).  User operators without a known identity
+// go through the generic kernels, which carry (value, present) pairs.
+
+template <class InputIt, class OutputIt, class BinaryOp, class UnaryOp>
+OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+                                  OutputIt d_first, BinaryOp binary_op, UnaryOp unary_op) {
+  return b2p_stdpar_detail::scan_call<true>("transform_inclusive_scan", first, last, d_first,
+                                            [binary_op, unary_op](auto &q, auto &g, auto a, auto b, auto o) {
+                                              hipsycl::algorithms::transform_inclusive_scan(q, g, a, b, o, binary_op,
+                                                                                            unary_op);
+                                            });
+}
+
+template <class InputIt, class OutputIt, class BinaryOp, class UnaryOp, class T>
+OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+                                  OutputIt d_first, BinaryOp binary_op, UnaryOp unary_op, T init) {
+  return b2p_stdpar_detail::scan_call<true>("transform_inclusive_scan", first, last, d_first,
+                                            [binary_op, unary_op, init](auto &q, auto &g, auto a, auto b, auto o) {
+                                              hipsycl::algorithms::transform_inclusive_scan(q, g, a, b, o, binary_op,
+                                                                                            unary_op, init);
+                                            });
+}
+
+template <class InputIt, class OutputIt, class T, class BinaryOp, class UnaryOp>
+OutputIt transform_exclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+                                  OutputIt d_first, T init, BinaryOp binary_op, UnaryOp unary_op) {
+  return b2p_stdpar_detail::scan_call<false>("transform_exclusive_scan", first, last, d_first,
+                                             [binary_op, unary_op, init](auto &q, auto &g, auto a, auto b, auto o) {
+                                               hipsycl::algorithms::transform_exclusive_scan(q, g, a, b, o, init,
+                                                                                             binary_op, unary_op);
+                                             });
 }
 
 // ---------------------------------------------------------------- copy_if

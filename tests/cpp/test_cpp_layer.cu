@@ -422,6 +422,21 @@ static void test_stdpar() {
     std::inclusive_scan(u.begin(), u.end(), ur.begin(), std::multiplies<unsigned>{}, 3u);
     std::inclusive_scan(pol, u.begin(), u.end(), uo.begin(), std::multiplies<unsigned>{}, 3u);
     CHECK(uo == ur, "stdpar inclusive_scan multiplies init 3 n=%zu", n);
+    // transform scans (pstl-impl/numeric.hpp:469-576): a known operator, and a
+    // user lambda without a known identity (generic kernels)
+    auto sq = [] __host__ __device__(int x) { return (long long)x * x; };
+    std::vector<long long> lo(n), lr(n);
+    std::transform_inclusive_scan(v.begin(), v.end(), lr.begin(), std::plus<long long>{}, sq);
+    std::transform_inclusive_scan(pol, v.begin(), v.end(), lo.begin(), std::plus<long long>{}, sq);
+    CHECK(lo == lr, "stdpar transform_inclusive_scan n=%zu", n);
+    auto keep_max = [] __host__ __device__(int a, int b) { return a < b ? b : a; };
+    auto wave = [] __host__ __device__(int x) { return (x * 7919) % 1000 - 500; };
+    std::transform_inclusive_scan(v.begin(), v.end(), ref.begin(), keep_max, wave, -600);
+    std::transform_inclusive_scan(pol, v.begin(), v.end(), out.begin(), keep_max, wave, -600);
+    CHECK(out == ref, "stdpar transform_inclusive_scan lambda op init n=%zu", n);
+    std::transform_exclusive_scan(v.begin(), v.end(), ref.begin(), 11, keep_max, wave);
+    std::transform_exclusive_scan(pol, v.begin(), v.end(), out.begin(), 11, keep_max, wave);
+    CHECK(out == ref, "stdpar transform_exclusive_scan lambda op n=%zu", n);
   }
   for (int mode = 0; mode < 3; ++mode) {
     std::vector<int> v(1000), out(1000, -1), ref;
