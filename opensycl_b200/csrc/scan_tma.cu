@@ -104,7 +104,7 @@ struct PipeState {
   long long tile[kMaxStages];
   // TMEM-staged scan: slot handed back by the emitters, output stage handed
   // back by the store warp, tile ids of input and output stages, TMEM base
-  uint64_t slot_free[kMaxStages], out_empty[kMaxStages];
+  uint64_t slot_free[kMaxStages], out_empty[kMaxStages], slot_ready[kMaxStages];
   long long tile_in[kMaxStages], tile_out[kMaxStages];
   unsigned long long out_carry[kMaxStages], out_count[kMaxStages];  // copy_if: output stage's position, count
   uint32_t tmem_base;
@@ -254,6 +254,40 @@ __device__ __forceinline__ typename Ops::Pub group_exclusive_scan(typename Ops::
   if (warp > 0) ex = Ops::combine(s_warp[warp - 1], ex);
   *total = s_warp[kWarps - 1];
   return ex;  // callers end with a bar_named(bar, NC) before s_warp is used again
+}
+
+// Exclusive scan over one warp group of NC threads with a single named
+// barrier: after the warp totals are in s_warp, every warp scans them itself
+// (the same combine tree warp 0 runs in group_exclusive_scan, so the same
+// bits).  s_warp may be written again only after a later barrier of the
+// group.
+template <class Ops, int NC>
+__device__ __forceinline__ typename Ops::Pub group_exclusive_scan_1bar(typename Ops::Pub v,
+                                                                       typename Ops::Pub *s_warp,
+                                                                       typename Ops::Pub *total, int t, int bar) {
+  using Pub = typename Ops::Pub;
+  constexpr int kWarps = NC / 32;
+  const int lane = t & 31, warp = t >> 5;
+  Pub incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    Pub o = shfl_up(incl, d);
+    if (lane >= d) incl = Ops::combine(o, incl);
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  bar_named(bar, NC);
+  Pub w = lane < kWarps ? s_warp[lane] : Ops::identity();
+#pragma unroll
+  for (int d = 1; d < kWarps; d <<= 1) {
+    Pub o = shfl_up(w, d);
+    if (lane >= d) w = Ops::combine(o, w);
+  }
+  const Pub before = shfl_idx(w, warp > 0 ? warp - 1 : 0);
+  *total = shfl_idx(w, kWarps - 1);
+  Pub ex = shfl_up(incl, 1);
+  if (lane == 0) ex = Ops::identity();
+  if (warp > 0) ex = Ops::combine(before, ex);
+  return ex;
 }
 
 // Carry of tile 0 (init, or the identity), in the published representation.
@@ -661,6 +695,7 @@ __device__ __forceinline__ void tmem_pipe_init(PipeState &ps, const TmaParams &p
       mbar_init(&ps.aggr[i], 1);
       mbar_init(&ps.cready[i], 1);
       mbar_init(&ps.slot_free[i], group_warps);
+      mbar_init(&ps.slot_ready[i], group_warps);
     }
     for (int i = 0; i < p.out_stages; ++i) {
       mbar_init(&ps.emitted[i], 1);
@@ -749,11 +784,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       tmem_st16(ta, w);
       if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
       Acc tile_agg;
-      texcl_all[(size_t)rs.s * NC + t] = group_exclusive_scan<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
-      tmem_wait_st();
-      tmem_fence_before();
-      bar_named(1, NC);  // slot and thread prefixes complete
-      if (t == 0) {
+      texcl_all[(size_t)rs.s * NC + t] = group_exclusive_scan_1bar<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
+      if (t == 0) {  // the aggregate goes out before the slot is complete
         const unsigned long long bits = publish_value<P, WIDE>(tile_agg);
         if (tile != p.stall_tile) {
           if (tile == 0)
@@ -766,6 +798,10 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         ps.agg[rs.s] = bits;
         mbar_arrive(&ps.aggr[rs.s]);
       }
+      tmem_wait_st();
+      tmem_fence_before();
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);  // this warp's slot columns and prefixes
     }
     if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
   } else if (warp < 2 * NC / 32) {
@@ -777,6 +813,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
     for (long long it = 0;; ++it, rs.advance(1, SL), ro.advance(1, SO)) {
       if (t == 0) {
         int go = emitter_wait(p, ps, rs, it);
+        if (go > 0 && !mbar_wait(&ps.slot_ready[rs.s], rs.ph, p.timeout_ns)) go = -1;
         if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
         if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         if (go == 0) {
