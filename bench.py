@@ -263,6 +263,7 @@ def main():
         "clocks": clocks,
         "per_kernel_ms": {"dot": round(dot_ms, 4), "scan": round(scan_ms, 4)},
         "dot_result": from_dot,
+        "precision": measure_precision(torch, a, b, x, y, dres),
     }
 
     if rank == 0 and world == 1:
@@ -426,9 +427,29 @@ def measure_e2e(C, torch, a_h, b_h, x_h, args):
                     "two buffer sets, step k's D2H overlaps step k+1's H2D"}
 
 
+def measure_precision(torch, a, b, x, y, dres):
+    """Error of the timed step's fp32 results against float64 on the device
+    (torch, outside the timed region): the dot relative and condition-normalised
+    (|got - ref| / sum |a_i b_i|) errors, the scan's largest relative error."""
+    ad, bd = a.double(), b.double()
+    prod = ad * bd
+    ref = float(prod.sum().item())
+    cond = float(prod.abs().sum().item())
+    del ad, bd, prod
+    got = float(dres.item())
+    ref_s = torch.cumsum(x.double(), 0)
+    rel_s = ((y.double() - ref_s).abs() / ref_s.abs().clamp_min(1e-300)).max().item()
+    del ref_s
+    return {"reference": "float64 on the device (torch)",
+            "dot_rel_err": abs(got - ref) / abs(ref), "dot_cond_err": abs(got - ref) / cond,
+            "scan_max_rel_err": rel_s, "tolerance": 1e-6}
+
+
 def cpu_baseline(a_h, b_h, x_h):
     """Oracle port of the OpenMP-backend evaluation order on the host cores,
     on a bounded sample (2^26 elements, ~10 s of CPU work at most)."""
+    import numpy as np
+
     from oracle import oracle as O
 
     ns = 1 << 26
@@ -443,8 +464,10 @@ def cpu_baseline(a_h, b_h, x_h):
         if time.perf_counter() - t0 > 8.0 or reps >= 20:
             break
     dt = time.perf_counter() - t0
+    got = float(O.dot(O.F32, a, b, 0.0))
+    ref = float(np.dot(a.astype(np.float64), b.astype(np.float64)))
     return {"value": round(16.0 * ns * reps / dt / 1e9, 3), "unit": "GB/s", "cores": threads,
-            "kind": "port",
+            "kind": "port", "dot_rel_err_vs_fp64": abs(got - ref) / abs(ref),
             "sample": f"{reps} x (dot + inclusive_scan) over 2^26 fp32 elements, "
                       f"OpenMP-backend evaluation order"}
 

@@ -20,6 +20,15 @@
 // (there is no host fallback); the per-operation history the reference
 // keeps for that decision (offload_heuristic_db.hpp:232-365) is recorded
 // and can be read with b2p_stdpar::offload_history().
+//
+// Offload front (offload.hpp:165-238, detail/stdpar_builtins.hpp:17-37):
+// managed (shared-USM) ranges are prefetched to the GPU on the call's stream
+// before the kernel; the policy b2p_stdpar::par_unseq_async leaves scans
+// non-blocking, as the reference's are, when no range needs staging: calls
+// queue back to back on the thread's in-order stream and
+// b2p_stdpar::sync() is the barrier the reference's compiler inserts before
+// host code reads the results.  reduce, transform_reduce and copy_if return
+// values and always block.
 #pragma once
 
 #include "algorithms.hpp"
@@ -31,8 +40,12 @@
 
 namespace b2p_stdpar {
 
-struct par_unseq_policy {};
+struct par_unseq_policy {
+  bool nonblocking_scans = false;
+};
 inline constexpr par_unseq_policy par_unseq{};
+// par_unseq whose scans return without waiting (see b2p_stdpar::sync)
+inline constexpr par_unseq_policy par_unseq_async{true};
 
 struct offload_record {
   std::string op;
@@ -59,6 +72,15 @@ auto raw(It it) {
   return &*it;
 }
 
+inline bool is_managed(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged;
+}
+
 // A device view of a contiguous range: the original pointer when the GPU
 // can reach it, otherwise a staged device copy (copied back by copy_back()).
 template <class T>
@@ -68,6 +90,11 @@ class view {
       : host_(p), n_(n), rt_(rt) {
     if (alg::detail::device_accessible(p)) {
       dev_ = p;
+      if (n && is_managed(p)) {  // pages move to the GPU ahead of the kernel
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaMemPrefetchAsync(p, n * sizeof(T), dev, rt.q.cuda_stream()) != cudaSuccess) cudaGetLastError();
+      }
     } else {
       dev_ = g.obtain<std::remove_cv_t<T>>(n ? n : 1);
       if (copy_in && n)
@@ -75,6 +102,7 @@ class view {
     }
   }
   T *get() const { return dev_; }
+  bool staged() const { return dev_ != host_; }
   void copy_back(size_t count) {
     if (dev_ != host_ && count) rt_.q.memcpy(const_cast<std::remove_cv_t<T> *>(host_), dev_, count * sizeof(T));
   }
@@ -115,8 +143,13 @@ T reduce_impl(const char *name, size_t n, F &&launch) {
 
 }  // namespace detail
 
-// Offload history of the calling thread: operation, size, seconds.
+// Offload history of the calling thread: operation, size, seconds (for
+// non-blocking scans, the time to enqueue).
 inline const std::vector<offload_record> &offload_history() { return detail::tls_runtime::get().history; }
+
+// Wait for every call this thread has offloaded (the barrier before host
+// code reads the results of par_unseq_async scans).
+inline void sync() { detail::tls_runtime::get().q.wait(); }
 
 }  // namespace b2p_stdpar
 
@@ -188,7 +221,8 @@ T transform_reduce(const b2p_stdpar::par_unseq_policy &, ForwardIt first, Forwar
 
 namespace b2p_stdpar_detail {
 template <bool INCL, class InputIt, class OutputIt, class Run>
-OutputIt scan_call(const char *name, InputIt first, InputIt last, OutputIt d_first, Run run) {
+OutputIt scan_call(const b2p_stdpar::par_unseq_policy &pol, const char *name, InputIt first, InputIt last,
+                   OutputIt d_first, Run run) {
   namespace d = b2p_stdpar::detail;
   const size_t n = (size_t)std::distance(first, last);
   if (n == 0) return d_first;
@@ -201,41 +235,41 @@ OutputIt scan_call(const char *name, InputIt first, InputIt last, OutputIt d_fir
   d::view<O> out(g, rt, d::raw(d_first), n, false);
   run(rt.q, g, in.get(), in.get() + n, out.get());
   out.copy_back(n);
-  rt.q.wait();
+  if (!pol.nonblocking_scans || in.staged() || out.staged()) rt.q.wait();
   return d_first + n;
 }
 }  // namespace b2p_stdpar_detail
 
 template <class InputIt, class OutputIt>
-OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first) {
-  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first, [](auto &q, auto &g, auto a,
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last, OutputIt d_first) {
+  return b2p_stdpar_detail::scan_call<true>(pol, "inclusive_scan", first, last, d_first, [](auto &q, auto &g, auto a,
                                                                                         auto b, auto o) {
     hipsycl::algorithms::inclusive_scan(q, g, a, b, o);
   });
 }
 
 template <class InputIt, class OutputIt, class BinaryOp>
-OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first,
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last, OutputIt d_first,
                         BinaryOp op) {
-  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first, [op](auto &q, auto &g, auto a,
+  return b2p_stdpar_detail::scan_call<true>(pol, "inclusive_scan", first, last, d_first, [op](auto &q, auto &g, auto a,
                                                                                           auto b, auto o) {
     hipsycl::algorithms::inclusive_scan(q, g, a, b, o, op);
   });
 }
 
 template <class InputIt, class OutputIt, class BinaryOp, class T>
-OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first,
+OutputIt inclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last, OutputIt d_first,
                         BinaryOp op, T init) {
-  return b2p_stdpar_detail::scan_call<true>("inclusive_scan", first, last, d_first,
+  return b2p_stdpar_detail::scan_call<true>(pol, "inclusive_scan", first, last, d_first,
                                             [op, init](auto &q, auto &g, auto a, auto b, auto o) {
                                               hipsycl::algorithms::inclusive_scan(q, g, a, b, o, op, init);
                                             });
 }
 
 template <class InputIt, class OutputIt, class T, class BinaryOp>
-OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last, OutputIt d_first, T init,
+OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last, OutputIt d_first, T init,
                         BinaryOp op) {
-  return b2p_stdpar_detail::scan_call<false>("exclusive_scan", first, last, d_first,
+  return b2p_stdpar_detail::scan_call<false>(pol, "exclusive_scan", first, last, d_first,
                                              [op, init](auto &q, auto &g, auto a, auto b, auto o) {
                                                hipsycl::algorithms::exclusive_scan(q, g, a, b, o, init, op);
                                              });
@@ -252,9 +286,9 @@ OutputIt exclusive_scan(const b2p_stdpar::par_unseq_policy &p, InputIt first, In
 // go through the generic kernels, which carry (value, present) pairs.
 
 template <class InputIt, class OutputIt, class BinaryOp, class UnaryOp>
-OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last,
                                   OutputIt d_first, BinaryOp binary_op, UnaryOp unary_op) {
-  return b2p_stdpar_detail::scan_call<true>("transform_inclusive_scan", first, last, d_first,
+  return b2p_stdpar_detail::scan_call<true>(pol, "transform_inclusive_scan", first, last, d_first,
                                             [binary_op, unary_op](auto &q, auto &g, auto a, auto b, auto o) {
                                               hipsycl::algorithms::transform_inclusive_scan(q, g, a, b, o, binary_op,
                                                                                             unary_op);
@@ -262,9 +296,9 @@ OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt 
 }
 
 template <class InputIt, class OutputIt, class BinaryOp, class UnaryOp, class T>
-OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last,
                                   OutputIt d_first, BinaryOp binary_op, UnaryOp unary_op, T init) {
-  return b2p_stdpar_detail::scan_call<true>("transform_inclusive_scan", first, last, d_first,
+  return b2p_stdpar_detail::scan_call<true>(pol, "transform_inclusive_scan", first, last, d_first,
                                             [binary_op, unary_op, init](auto &q, auto &g, auto a, auto b, auto o) {
                                               hipsycl::algorithms::transform_inclusive_scan(q, g, a, b, o, binary_op,
                                                                                             unary_op, init);
@@ -272,9 +306,9 @@ OutputIt transform_inclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt 
 }
 
 template <class InputIt, class OutputIt, class T, class BinaryOp, class UnaryOp>
-OutputIt transform_exclusive_scan(const b2p_stdpar::par_unseq_policy &, InputIt first, InputIt last,
+OutputIt transform_exclusive_scan(const b2p_stdpar::par_unseq_policy &pol, InputIt first, InputIt last,
                                   OutputIt d_first, T init, BinaryOp binary_op, UnaryOp unary_op) {
-  return b2p_stdpar_detail::scan_call<false>("transform_exclusive_scan", first, last, d_first,
+  return b2p_stdpar_detail::scan_call<false>(pol, "transform_exclusive_scan", first, last, d_first,
                                              [binary_op, unary_op, init](auto &q, auto &g, auto a, auto b, auto o) {
                                                hipsycl::algorithms::transform_exclusive_scan(q, g, a, b, o, init,
                                                                                              binary_op, unary_op);

@@ -448,6 +448,31 @@ static void test_stdpar() {
     CHECK((size_t)(end - out.begin()) == ref.size(), "stdpar copy_if mode %d count", mode);
     CHECK(std::equal(ref.begin(), ref.end(), out.begin()), "stdpar copy_if mode %d values", mode);
   }
+  // managed (shared-USM) ranges: prefetched, and with par_unseq_async the
+  // scans queue back to back until b2p_stdpar::sync()
+  {
+    const size_t n = (1u << 20) + 3;
+    int *m = nullptr, *o1 = nullptr, *o2 = nullptr;
+    CHECK(cudaMallocManaged(&m, n * sizeof(int)) == cudaSuccess, "cudaMallocManaged");
+    cudaMallocManaged(&o1, n * sizeof(int));
+    cudaMallocManaged(&o2, n * sizeof(int));
+    for (size_t i = 0; i < n; ++i) m[i] = (int)(i % 13) - 6;
+    std::vector<int> r1(n), r2(n);
+    std::inclusive_scan(m, m + n, r1.begin());
+    std::exclusive_scan(r1.begin(), r1.end(), r2.begin(), 4);
+    const auto &apol = b2p_stdpar::par_unseq_async;
+    std::inclusive_scan(apol, m, m + n, o1);
+    std::exclusive_scan(apol, o1, o1 + n, o2, 4);  // ordered after the first on the thread's stream
+    b2p_stdpar::sync();
+    CHECK(std::equal(r1.begin(), r1.end(), o1), "stdpar async inclusive_scan (managed)");
+    CHECK(std::equal(r2.begin(), r2.end(), o2), "stdpar async exclusive_scan after it (managed)");
+    std::inclusive_scan(apol, m, m + n, o1);
+    const long long red = std::reduce(pol, o1, o1 + n, 0ll);  // blocking, after the async scan
+    CHECK(red == std::accumulate(r1.begin(), r1.end(), 0ll), "stdpar reduce after async scan");
+    cudaFree(m);
+    cudaFree(o1);
+    cudaFree(o2);
+  }
   CHECK(!b2p_stdpar::offload_history().empty(), "stdpar offload history recorded");
 }
 
