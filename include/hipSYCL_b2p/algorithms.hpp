@@ -1,7 +1,8 @@
 // Drop-in for AdaptiveCpp's algorithms library on the data-parallel
 // primitive path: hipsycl::algorithms::{reduce, transform_reduce,
 // inclusive_scan, exclusive_scan, transform_inclusive_scan,
-// transform_exclusive_scan, copy_if} and util::{allocation_cache,
+// transform_exclusive_scan, copy_if, any_of, all_of, none_of} and
+// util::{allocation_cache,
 // allocation_group}, with the reference's signatures
 // (algorithms/numeric.hpp:170-327, algorithms/algorithm.hpp:178-243,
 // algorithms/util/allocation_cache.hpp:42-181) and semantics:
@@ -715,6 +716,90 @@ b2p_sycl::event copy_if(b2p_sycl::queue &q, util::allocation_group &scratch, For
   detail::tile_compact_kernel<<<(unsigned)ntiles, detail::kGB, 0, q.cuda_stream()>>>(n, first, pred, cnt, d_first);
   b2p_sycl::detail::check_cuda(cudaGetLastError(), "copy_if");
   return q.record();
+}
+
+// ----------------------------------------------- any_of / all_of / none_of
+// (algorithm.hpp:422-516).  *out receives 1 or 0; for first == last nothing
+// is launched and *out is left as it is, as in the reference.  The search
+// stops early: a warp that finds a hit raises a flag in *out, and every warp
+// looks at the flag before each stride of 8 elements per thread.
+
+namespace detail {
+using early_exit_flag_t = int;
+
+constexpr int kEarlyUnroll = 8;
+
+template <class It, class Pred>
+__global__ void __launch_bounds__(kGB) early_exit_kernel(size_t n, It first, Pred pred, bool negate,
+                                                           early_exit_flag_t *flag) {
+  const size_t span = (size_t)kGB * kEarlyUnroll;
+  for (size_t base = (size_t)blockIdx.x * span; base < n; base += (size_t)gridDim.x * span) {
+    int stop = 0;
+    if ((threadIdx.x & 31) == 0) stop = *reinterpret_cast<volatile early_exit_flag_t *>(flag);
+    if (__shfl_sync(0xffffffffu, stop, 0)) return;
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < kEarlyUnroll; ++k) {
+      const size_t j = base + (size_t)k * kGB + threadIdx.x;
+      if (j < n) {
+        const bool v = static_cast<bool>(pred(first[j]));
+        hit |= negate ? !v : v;
+      }
+    }
+    if (__any_sync(0xffffffffu, hit)) {
+      if ((threadIdx.x & 31) == 0) atomicExch(flag, 1);
+      return;
+    }
+  }
+}
+
+template <int = 0>
+__global__ void flip_flag_kernel(early_exit_flag_t *flag) {
+  *flag = !*flag;
+}
+
+// *out = 1 if some element satisfies pred (negate: fails it), else 0.
+template <class It, class Pred>
+b2p_sycl::event early_exit_search(b2p_sycl::queue &q, It first, size_t n, early_exit_flag_t *out, Pred pred,
+                                  bool negate, bool flip) {
+  require_device(first, "early-exit search");
+  require_device(out, "early-exit flag");
+  b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+  b2p_sycl::detail::check_cuda(cudaMemsetAsync(out, 0, sizeof(early_exit_flag_t), q.cuda_stream()), "memset");
+  int sms = 0, dev = q.get_device().cuda_ordinal();
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t span = (size_t)kGB * kEarlyUnroll;
+  const size_t want = (n + span - 1) / span;
+  const unsigned grid = (unsigned)std::min<size_t>(want, (size_t)std::max(sms, 1) * 8);
+  early_exit_kernel<<<grid, kGB, 0, q.cuda_stream()>>>(n, first, pred, negate, out);
+  if (flip) flip_flag_kernel<><<<1, 1, 0, q.cuda_stream()>>>(out);
+  b2p_sycl::detail::check_cuda(cudaGetLastError(), "early-exit search");
+  return q.record();
+}
+}  // namespace detail
+
+template <class ForwardIt, class UnaryPredicate>
+b2p_sycl::event any_of(b2p_sycl::queue &q, ForwardIt first, ForwardIt last, detail::early_exit_flag_t *out,
+                       UnaryPredicate p, const std::vector<b2p_sycl::event> &deps = {}) {
+  if (first == last) return b2p_sycl::event{};
+  q.depends_on(deps);
+  return detail::early_exit_search(q, first, (size_t)std::distance(first, last), out, p, false, false);
+}
+
+template <class ForwardIt, class UnaryPredicate>
+b2p_sycl::event all_of(b2p_sycl::queue &q, ForwardIt first, ForwardIt last, detail::early_exit_flag_t *out,
+                       UnaryPredicate p, const std::vector<b2p_sycl::event> &deps = {}) {
+  if (first == last) return b2p_sycl::event{};
+  q.depends_on(deps);
+  return detail::early_exit_search(q, first, (size_t)std::distance(first, last), out, p, true, true);
+}
+
+template <class ForwardIt, class UnaryPredicate>
+b2p_sycl::event none_of(b2p_sycl::queue &q, ForwardIt first, ForwardIt last, detail::early_exit_flag_t *out,
+                        UnaryPredicate p, const std::vector<b2p_sycl::event> &deps = {}) {
+  if (first == last) return b2p_sycl::event{};
+  q.depends_on(deps);
+  return detail::early_exit_search(q, first, (size_t)std::distance(first, last), out, p, false, true);
 }
 
 }  // namespace algorithms

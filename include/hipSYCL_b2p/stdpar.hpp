@@ -1,7 +1,8 @@
 // Offloaded C++ standard parallel algorithms on the primitive path:
 // std::reduce (3 overloads), std::transform_reduce (3), std::inclusive_scan
 // (3), std::exclusive_scan (2), std::transform_inclusive_scan (2),
-// std::transform_exclusive_scan (1) and std::copy_if, taking the execution
+// std::transform_exclusive_scan (1), std::copy_if and std::any_of / all_of
+// / none_of, taking the execution
 // policy b2p_stdpar::par_unseq (AdaptiveCpp: the par_unseq overloads of
 // std/stdpar/pstl-impl/numeric.hpp:28-576 and pstl-impl/algorithm.hpp:150-187,
 // which its compiler pass substitutes for std::execution::par_unseq; here
@@ -313,6 +314,51 @@ OutputIt transform_exclusive_scan(const b2p_stdpar::par_unseq_policy &pol, Input
                                                hipsycl::algorithms::transform_exclusive_scan(q, g, a, b, o, init,
                                                                                              binary_op, unary_op);
                                              });
+}
+
+// ----------------------------------------------------- any / all / none
+// (pstl-impl/algorithm.hpp:403-500): blocking, empty ranges give the
+// standard answers without a launch.
+
+namespace b2p_stdpar_detail {
+template <class ForwardIt, class Call>
+bool flag_call(const char *name, ForwardIt first, ForwardIt last, bool empty_answer, Call call) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return empty_answer;
+  d::timer tm(name, n);
+  auto &rt = d::tls_runtime::get();
+  hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
+  using V = typename std::iterator_traits<ForwardIt>::value_type;
+  d::view<const V> in(g, rt, d::raw(first), n, true);
+  int *flag = g.obtain<int>(1);
+  call(rt.q, in.get(), in.get() + n, flag);
+  int r = 0;
+  rt.q.memcpy(&r, flag, sizeof(int));
+  rt.q.wait();
+  return r != 0;
+}
+}  // namespace b2p_stdpar_detail
+
+template <class ForwardIt, class UnaryPredicate>
+bool any_of(const b2p_stdpar::par_unseq_policy &, ForwardIt first, ForwardIt last, UnaryPredicate p) {
+  return b2p_stdpar_detail::flag_call("any_of", first, last, false, [p](auto &q, auto a, auto b, int *f) {
+    hipsycl::algorithms::any_of(q, a, b, f, p);
+  });
+}
+
+template <class ForwardIt, class UnaryPredicate>
+bool all_of(const b2p_stdpar::par_unseq_policy &, ForwardIt first, ForwardIt last, UnaryPredicate p) {
+  return b2p_stdpar_detail::flag_call("all_of", first, last, true, [p](auto &q, auto a, auto b, int *f) {
+    hipsycl::algorithms::all_of(q, a, b, f, p);
+  });
+}
+
+template <class ForwardIt, class UnaryPredicate>
+bool none_of(const b2p_stdpar::par_unseq_policy &, ForwardIt first, ForwardIt last, UnaryPredicate p) {
+  return b2p_stdpar_detail::flag_call("none_of", first, last, true, [p](auto &q, auto a, auto b, int *f) {
+    hipsycl::algorithms::none_of(q, a, b, f, p);
+  });
 }
 
 // ---------------------------------------------------------------- copy_if

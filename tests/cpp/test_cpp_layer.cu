@@ -179,6 +179,31 @@ static void test_algorithms(sycl::queue &q) {
     sycl::free(neg, q);
     sycl::free(fo, q);
   }
+  // any_of / all_of / none_of with the reference's signatures (no scratch,
+  // int flag; an empty range leaves *out alone)
+  {
+    const size_t n = (1ul << 23) + 11;
+    std::vector<int> h(n);
+    std::iota(h.begin(), h.end(), 0);
+    int *d = to_dev(q, h);
+    int *flag = sycl::malloc_shared<int>(1, q);
+    for (long long needle : {0ll, 12345ll, (long long)n - 1, -1ll}) {
+      auto eq = [needle] __host__ __device__(int x) { return (long long)x == needle; };
+      auto lt = [needle] __host__ __device__(int x) { return (long long)x < needle + 1; };
+      const bool found = needle >= 0;
+      alg::any_of(q, d, d + n, flag, eq).wait();
+      CHECK(*flag == (int)found, "any_of needle %lld got %d", needle, *flag);
+      alg::none_of(q, d, d + n, flag, eq).wait();
+      CHECK(*flag == (int)!found, "none_of needle %lld got %d", needle, *flag);
+      alg::all_of(q, d, d + n, flag, lt).wait();
+      CHECK(*flag == (int)(needle == (long long)n - 1), "all_of below %lld got %d", needle, *flag);
+    }
+    *flag = 42;
+    alg::any_of(q, d, d, flag, [] __host__ __device__(int) { return true; }).wait();
+    CHECK(*flag == 42, "any_of of an empty range touched *out");
+    sycl::free(d, q);
+    sycl::free(flag, q);
+  }
   // the cache reuses its allocations
   {
     int *d = to_dev(q, std::vector<int>(5000, 1));
@@ -472,6 +497,28 @@ static void test_stdpar() {
     cudaFree(m);
     cudaFree(o1);
     cudaFree(o2);
+  }
+  // any_of / all_of / none_of (algorithm.hpp:422-516, pstl-impl/algorithm.hpp:403-500)
+  for (size_t n : {1ul, 1000ul, (1ul << 22) + 7}) {
+    std::vector<int> v(n);
+    std::iota(v.begin(), v.end(), 0);
+    for (long long needle : {0ll, (long long)n / 2, (long long)n - 1, -5ll}) {
+      auto eq = [needle] __host__ __device__(int x) { return (long long)x == needle; };
+      auto ne = [needle] __host__ __device__(int x) { return (long long)x != needle; };
+      CHECK(std::any_of(pol, v.begin(), v.end(), eq) == std::any_of(v.begin(), v.end(), eq),
+            "stdpar any_of n=%zu needle=%lld", n, needle);
+      CHECK(std::all_of(pol, v.begin(), v.end(), ne) == std::all_of(v.begin(), v.end(), ne),
+            "stdpar all_of n=%zu needle=%lld", n, needle);
+      CHECK(std::none_of(pol, v.begin(), v.end(), eq) == std::none_of(v.begin(), v.end(), eq),
+            "stdpar none_of n=%zu needle=%lld", n, needle);
+    }
+  }
+  {
+    std::vector<int> e;
+    auto any = [] __host__ __device__(int) { return true; };
+    CHECK(!std::any_of(pol, e.begin(), e.end(), any) && std::all_of(pol, e.begin(), e.end(), any) &&
+              std::none_of(pol, e.begin(), e.end(), any),
+          "stdpar any/all/none of an empty range");
   }
   CHECK(!b2p_stdpar::offload_history().empty(), "stdpar offload history recorded");
 }
