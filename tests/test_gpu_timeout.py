@@ -26,11 +26,12 @@ def short_timeout():
 
 @pytest.mark.parametrize("prim", ["scan", "copy_if"])
 # look-back kernel (128 x 4 tiles) / two-phase kernel (128 x 4) / pipelined
-# TMA scan (256 x 32 = 8192-element tiles; copy_if runs two-phase there)
-@pytest.mark.parametrize("config,stall", [(0, 37), (16, 37), (23, 5)])
-def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, config, stall):
+# TMEM-staged scan and copy_if (256 x 32 = 8192-element tiles), with one
+# tile per block and with several (the rings of stages and TMEM slots wrap)
+@pytest.mark.parametrize("config,stall,n", [(0, 37, 512 * 200), (16, 37, 512 * 200), (23, 5, 512 * 200),
+                                            (23, 150, 8192 * 400 + 77)])
+def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, config, stall, n):
     L = C.lib()
-    n = 512 * 200
     x = torch.arange(n, dtype=torch.int32, device="cuda")
     C.device_error(clear=True)
     L.b2p_debug_stall_tile(stall)
@@ -46,6 +47,6 @@ def test_stalled_tile_times_out_and_context_survives(dev, short_timeout, prim, c
     assert dt < 30.0
     # the same scratch and context keep working
     y = C.scan(x, True, "sum", None, config=config)
-    ref = np.cumsum(np.arange(n, dtype=np.int64)).astype(np.int32)
+    ref = (np.cumsum(np.arange(n, dtype=np.int64)) & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
     assert np.array_equal(y.cpu().numpy(), ref)
     assert C.device_error(clear=True) == C.OK
