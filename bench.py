@@ -472,6 +472,20 @@ def cpu_baseline(a_h, b_h, x_h):
                       f"OpenMP-backend evaluation order"}
 
 
+def _time_b2b(torch, fn, reps=10, warm=3):
+    """Mean time of `reps` back-to-back launches between one event pair."""
+    s = torch.cuda.current_stream()
+    for _ in range(warm):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def _time_op(torch, fn, reps=10, warm=3, flush=None):
     s = torch.cuda.current_stream()
     for _ in range(warm):
@@ -494,10 +508,17 @@ def measure_ops(C, torch, np, peak):
     ops = {}
     n = N28
 
-    def rec(name, ms, nbytes, note=None):
+    def rec(name, fn, nbytes, note=None, flush=None):
+        """Median of single launches (an event pair around each launch), and
+        for inputs larger than L2 also the mean of 10 back-to-back launches."""
+        ms = _time_op(torch, fn, flush=flush)
         gbs = nbytes / (ms / 1e3) / 1e9
         ops[name] = {"ms": round(ms, 4), "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
                      "bytes": nbytes}
+        if flush is None:
+            b2b = nbytes / (_time_b2b(torch, fn) / 1e3) / 1e9
+            ops[name]["b2b_GB/s"] = round(b2b, 1)
+            ops[name]["b2b_frac_hbm"] = round(b2b / peak, 4)
         if note:
             ops[name]["note"] = note
 
@@ -505,42 +526,42 @@ def measure_ops(C, torch, np, peak):
     xi = torch.from_numpy(C.synth_fill(0, 0, n, -1000, 1000)).cuda()
     yi = torch.empty_like(xi)
     out = torch.zeros(1, dtype=torch.int32, device="cuda")
-    rec("reduce_i32_2^28", _time_op(torch, lambda: C.reduce(xi, "sum", init=0, out=out)), 4 * n)
-    rec("scan_i32_2^28", _time_op(torch, lambda: C.scan(xi, True, "sum", None, out=yi)), 8 * n)
+    rec("reduce_i32_2^28", lambda: C.reduce(xi, "sum", init=0, out=out), 4 * n)
+    rec("scan_i32_2^28", lambda: C.scan(xi, True, "sum", None, out=yi), 8 * n)
     x24 = xi[:N24]
     y24 = yi[:N24]
-    rec("reduce_i32_2^24_flushed", _time_op(torch, lambda: C.reduce(x24, "sum", init=0, out=out), flush=flush),
-        4 * N24, "L2 flushed before each rep")
-    rec("scan_i32_2^24_flushed", _time_op(torch, lambda: C.scan(x24, True, "sum", None, out=y24), flush=flush),
-        8 * N24, "L2 flushed before each rep")
+    rec("reduce_i32_2^24_flushed", lambda: C.reduce(x24, "sum", init=0, out=out), 4 * N24,
+        "L2 flushed before each rep", flush=flush)
+    rec("scan_i32_2^24_flushed", lambda: C.scan(x24, True, "sum", None, out=y24), 8 * N24,
+        "L2 flushed before each rep", flush=flush)
     del xi, yi
     xf = torch.from_numpy(C.synth_fill(1, 1, n, 0.125, 1e-6)).cuda()
     bf = torch.from_numpy(C.synth_fill(1, 2, n, 0.125, 1e-6)).cuda()
     of = torch.zeros(1, dtype=torch.float32, device="cuda")
-    rec("reduce_f32_2^28", _time_op(torch, lambda: C.reduce(xf, "sum", init=0.0, out=of)), 4 * n)
-    rec("dot_f32_2^28", _time_op(torch, lambda: C.dot(xf, bf, out=of)), 8 * n)
+    rec("reduce_f32_2^28", lambda: C.reduce(xf, "sum", init=0.0, out=of), 4 * n)
+    rec("dot_f32_2^28", lambda: C.dot(xf, bf, out=of), 8 * n)
     yf = torch.empty_like(xf)
-    rec("scan_f32_2^28", _time_op(torch, lambda: C.scan(xf, True, "sum", None, out=yf)), 8 * n)
+    rec("scan_f32_2^28", lambda: C.scan(xf, True, "sum", None, out=yf), 8 * n)
     del bf
     ab = torch.from_numpy(C.synth_fill(6, 1, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
     bb = torch.from_numpy(C.synth_fill(6, 2, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
-    rec("dot_bf16_2^28", _time_op(torch, lambda: C.dot(ab, bb, out=of)), 4 * n)
-    rec("scan_bf16in_f32out_2^28", _time_op(torch, lambda: C.scan(ab, True, "sum", None, out=yf)), 6 * n)
+    rec("dot_bf16_2^28", lambda: C.dot(ab, bb, out=of), 4 * n)
+    rec("scan_bf16in_f32out_2^28", lambda: C.scan(ab, True, "sum", None, out=yf), 6 * n)
     del ab, bb, xf, yf
     xu = torch.from_numpy(C.synth_fill(3, 4, n)).cuda()
     yu = torch.empty_like(xu)
-    rec("exclusive_scan_u32_2^28", _time_op(torch, lambda: C.scan(xu, False, "sum", 0, out=yu)), 8 * n)
+    rec("exclusive_scan_u32_2^28", lambda: C.scan(xu, False, "sum", 0, out=yu), 8 * n)
     cnt = C.zeros(1, torch.uint64, "cuda")
     C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt)
     kept = int(cnt.item())
-    rec("copy_if_u32_2^28", _time_op(torch, lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt)),
+    rec("copy_if_u32_2^28", lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt),
         4 * n + 4 * kept, f"kept {kept} ({kept / n:.4f})")
     del xu, yu
     k = torch.from_numpy(C.synth_fill(4, 5, n, 1.2)).cuda()
     bins = torch.zeros(256, dtype=torch.int32, device="cuda")
-    rec("histogram_u8_zipf1.2_2^28", _time_op(torch, lambda: C.histogram_u8(k, bins=bins)), n + 1024)
+    rec("histogram_u8_zipf1.2_2^28", lambda: C.histogram_u8(k, bins=bins), n + 1024)
     ku = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda")
-    rec("histogram_u8_uniform_2^28", _time_op(torch, lambda: C.histogram_u8(ku, bins=bins)), n + 1024)
+    rec("histogram_u8_uniform_2^28", lambda: C.histogram_u8(ku, bins=bins), n + 1024)
     return ops
 
 
