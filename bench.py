@@ -154,6 +154,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--log2n", type=int, default=28,
                     help="elements per array of the headline step (small cases for profiling)")
+    ap.add_argument("--ops-log2n", type=int, default=28,
+                    help="elements per array of the per-primitive table (below 28: no 2^24, segmented "
+                         "or selector entries; small cases for profiling)")
+    ap.add_argument("--ops-reps", type=int, default=10, help="timed launches per primitive")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -271,9 +275,10 @@ def main():
         if not args.no_cpu:
             result["cpu_baseline"] = cpu_baseline(a_h, b_h, x_h)
         if not args.no_ops:
-            result["ops"] = measure_ops(C, torch, np, peak)
-            result["segmented"] = measure_segmented(C, torch, np, peak)
-            result["selector"] = measure_selector_stream(selector_state)
+            result["ops"] = measure_ops(C, torch, np, peak, args.ops_log2n, args.ops_reps)
+            if args.ops_log2n == 28:
+                result["segmented"] = measure_segmented(C, torch, np, peak)
+                result["selector"] = measure_selector_stream(selector_state)
         result["selector_state"] = selector_state["status"]
     else:
         result["e2e"] = None
@@ -503,20 +508,22 @@ def _time_op(torch, fn, reps=10, warm=3, flush=None):
     return statistics.median(ts)
 
 
-def measure_ops(C, torch, np, peak):
-    """Per-primitive GB/s and fraction of measured HBM peak."""
+def measure_ops(C, torch, np, peak, log2n=28, reps=10):
+    """Per-primitive GB/s and fraction of measured HBM peak on arrays of
+    2^log2n elements."""
     ops = {}
-    n = N28
+    n = 1 << log2n
+    sz = f"2^{log2n}"
 
     def rec(name, fn, nbytes, note=None, flush=None):
         """Median of single launches (an event pair around each launch), and
         for inputs larger than L2 also the mean of 10 back-to-back launches."""
-        ms = _time_op(torch, fn, flush=flush)
+        ms = _time_op(torch, fn, reps=reps, flush=flush)
         gbs = nbytes / (ms / 1e3) / 1e9
         ops[name] = {"ms": round(ms, 4), "GB/s": round(gbs, 1), "frac_hbm": round(gbs / peak, 4),
                      "bytes": nbytes}
         if flush is None:
-            b2b = nbytes / (_time_b2b(torch, fn) / 1e3) / 1e9
+            b2b = nbytes / (_time_b2b(torch, fn, reps=reps) / 1e3) / 1e9
             ops[name]["b2b_GB/s"] = round(b2b, 1)
             ops[name]["b2b_frac_hbm"] = round(b2b / peak, 4)
         if note:
@@ -526,42 +533,43 @@ def measure_ops(C, torch, np, peak):
     xi = torch.from_numpy(C.synth_fill(0, 0, n, -1000, 1000)).cuda()
     yi = torch.empty_like(xi)
     out = torch.zeros(1, dtype=torch.int32, device="cuda")
-    rec("reduce_i32_2^28", lambda: C.reduce(xi, "sum", init=0, out=out), 4 * n)
-    rec("scan_i32_2^28", lambda: C.scan(xi, True, "sum", None, out=yi), 8 * n)
-    x24 = xi[:N24]
-    y24 = yi[:N24]
-    rec("reduce_i32_2^24_flushed", lambda: C.reduce(x24, "sum", init=0, out=out), 4 * N24,
-        "L2 flushed before each rep", flush=flush)
-    rec("scan_i32_2^24_flushed", lambda: C.scan(x24, True, "sum", None, out=y24), 8 * N24,
-        "L2 flushed before each rep", flush=flush)
+    rec(f"reduce_i32_{sz}", lambda: C.reduce(xi, "sum", init=0, out=out), 4 * n)
+    rec(f"scan_i32_{sz}", lambda: C.scan(xi, True, "sum", None, out=yi), 8 * n)
+    if log2n == 28:
+        x24 = xi[:N24]
+        y24 = yi[:N24]
+        rec("reduce_i32_2^24_flushed", lambda: C.reduce(x24, "sum", init=0, out=out), 4 * N24,
+            "L2 flushed before each rep", flush=flush)
+        rec("scan_i32_2^24_flushed", lambda: C.scan(x24, True, "sum", None, out=y24), 8 * N24,
+            "L2 flushed before each rep", flush=flush)
     del xi, yi
     xf = torch.from_numpy(C.synth_fill(1, 1, n, 0.125, 1e-6)).cuda()
     bf = torch.from_numpy(C.synth_fill(1, 2, n, 0.125, 1e-6)).cuda()
     of = torch.zeros(1, dtype=torch.float32, device="cuda")
-    rec("reduce_f32_2^28", lambda: C.reduce(xf, "sum", init=0.0, out=of), 4 * n)
-    rec("dot_f32_2^28", lambda: C.dot(xf, bf, out=of), 8 * n)
+    rec(f"reduce_f32_{sz}", lambda: C.reduce(xf, "sum", init=0.0, out=of), 4 * n)
+    rec(f"dot_f32_{sz}", lambda: C.dot(xf, bf, out=of), 8 * n)
     yf = torch.empty_like(xf)
-    rec("scan_f32_2^28", lambda: C.scan(xf, True, "sum", None, out=yf), 8 * n)
+    rec(f"scan_f32_{sz}", lambda: C.scan(xf, True, "sum", None, out=yf), 8 * n)
     del bf
     ab = torch.from_numpy(C.synth_fill(6, 1, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
     bb = torch.from_numpy(C.synth_fill(6, 2, n, 0.125, 1e-6).view(np.int16)).cuda().view(torch.bfloat16)
-    rec("dot_bf16_2^28", lambda: C.dot(ab, bb, out=of), 4 * n)
-    rec("scan_bf16in_f32out_2^28", lambda: C.scan(ab, True, "sum", None, out=yf), 6 * n)
+    rec(f"dot_bf16_{sz}", lambda: C.dot(ab, bb, out=of), 4 * n)
+    rec(f"scan_bf16in_f32out_{sz}", lambda: C.scan(ab, True, "sum", None, out=yf), 6 * n)
     del ab, bb, xf, yf
     xu = torch.from_numpy(C.synth_fill(3, 4, n)).cuda()
     yu = torch.empty_like(xu)
-    rec("exclusive_scan_u32_2^28", lambda: C.scan(xu, False, "sum", 0, out=yu), 8 * n)
+    rec(f"exclusive_scan_u32_{sz}", lambda: C.scan(xu, False, "sum", 0, out=yu), 8 * n)
     cnt = C.zeros(1, torch.uint64, "cuda")
     C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt)
     kept = int(cnt.item())
-    rec("copy_if_u32_2^28", lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt),
+    rec(f"copy_if_u32_{sz}", lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt),
         4 * n + 4 * kept, f"kept {kept} ({kept / n:.4f})")
     del xu, yu
     k = torch.from_numpy(C.synth_fill(4, 5, n, 1.2)).cuda()
     bins = torch.zeros(256, dtype=torch.int32, device="cuda")
-    rec("histogram_u8_zipf1.2_2^28", lambda: C.histogram_u8(k, bins=bins), n + 1024)
+    rec(f"histogram_u8_zipf1.2_{sz}", lambda: C.histogram_u8(k, bins=bins), n + 1024)
     ku = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda")
-    rec("histogram_u8_uniform_2^28", lambda: C.histogram_u8(ku, bins=bins), n + 1024)
+    rec(f"histogram_u8_uniform_{sz}", lambda: C.histogram_u8(ku, bins=bins), n + 1024)
     return ops
 
 
