@@ -8,11 +8,18 @@ larger than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 (under torchrun): every rank runs its own replica of the step on its
-own GPU (weak scaling, no collective in the data path); the time is the max
-over ranks.  --impl reference times the reference algorithm's CPU
-implementation (the oracle port of the OpenMP backend's evaluation order)
-on the host cores, on a bounded sample of the same workload.
+N > 1 (under torchrun): the arrays are shards of one logical array of
+2^28 * N elements (rank r holds the r-th 2^28 elements).  The step is the
+sharded dot (local dot, all-gather of the N partials over NCCL) and the
+sharded inclusive scan (local reduce, all-gather of the N shard totals,
+local scan with the carry as init): weak scaling, time = max over ranks.
+--impl reference times the oracle's restatement of the reference's OpenMP
+backend (oracle/baseline.py) on the host cores, on the same workload; it
+loads nothing from this package.
+
+Before the headline line, compact JSON lines carry the per-primitive table
+(`ops_summary`), the segmented batch (`segmented_summary`) and the selector
+stream (`selector_summary`); the headline repeats their key figures.
 """
 from __future__ import annotations
 
@@ -102,42 +109,38 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- reference arm
 
-def run_reference(args):
-    import numpy as np
+def workload_config(log2n: int, world: int) -> dict:
+    n = 1 << log2n
+    return {"workload": f"fp32 dot(a,b) 2^{log2n} + fp32 inclusive_scan 2^{log2n}"
+                        + (f" per rank, one logical array of 2^{log2n} x {world}" if world > 1 else ""),
+            "elements": n, "step_bytes": 16.0 * n,
+            "l2": f"inputs ({12.0 * n / 2**30:g} GiB) larger than the 126 MB L2; no flush" if n >= N24
+                  else "inputs smaller than L2 (profiling size); no flush",
+            "parallelism": "single device" if world == 1 else f"sharded x{world} (one exchange per primitive)"}
 
-    from opensycl_b200 import capi as C
-    from oracle import oracle as O
 
-    ns = 1 << 26  # bounded sample: 1/4 of the 2^28 workload per step
-    a = C.synth_fill(1, 1, ns, 0.125, 1e-6)
-    b = C.synth_fill(1, 2, ns, 0.125, 1e-6)
-    x = C.synth_fill(2, 3, ns, 0.125, 1e-6)
-    threads = O.num_threads()
-    step_bytes = 16.0 * ns
+def run_reference(args, world):
+    """The oracle's restatement of the reference's OpenMP backend on every
+    host core, on the same workload as our arm (oracle/baseline.py, its own
+    process and generator: nothing from this package is loaded)."""
+    from oracle import baseline
 
-    def step():
-        O.dot(O.F32, a, b, 0.0)
-        O.scan(O.F32, O.SUM, True, x)
-
-    for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    dt = time.perf_counter() - t0
-    v = step_bytes * args.steps / dt / 1e9
+    r = baseline.run(args.log2n, args.steps, args.warmup)
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s",
+        "impl": "reference", "metric": METRIC, "value": round(r["value"], 3), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "ms_per_step": round(r["ms_per_step"], 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "fp32 dot(2^28) + inclusive_scan(2^28), sample 2^26 per step",
-                   "sample_elems": ns},
-        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"dot + inclusive_scan over 2^26 fp32 elements per step, "
-                                   f"OpenMP-backend evaluation order, {threads} threads"},
-        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+        "config": workload_config(args.log2n, world),
+        "cpu_baseline": {"value": round(r["value"], 3), "unit": "GB/s", "cores": r["threads"], "kind": "port",
+                         "cpu_model": r["cpu_model"], "omp": r["omp"],
+                         "sample": f"the full workload: {args.steps} timed steps of dot + inclusive_scan over "
+                                   f"2^{args.log2n} fp32 elements, OpenMP-backend evaluation order, "
+                                   f"{r['threads']} threads"},
+        "e2e": {"value": round(r["value"], 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "precision": {"dot_rel_err_vs_fp64": r["dot_rel_err_vs_fp64"],
+                      "scan_max_rel_err_vs_fp64": r["scan_max_rel_err_vs_fp64"]},
     }
     print(json.dumps(line), flush=True)
 
@@ -168,13 +171,14 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        run_reference(args)
+        run_reference(args, world)
         return
 
     import numpy as np
     import torch
 
     from opensycl_b200 import capi as C
+    from opensycl_b200 import sharded as SH
 
     torch.cuda.set_device(local)
     dist = None
@@ -192,6 +196,7 @@ def main():
     peak, peak_kind = hbm_peak()
     selector_state = install_selector(C)
     n = 1 << args.log2n
+    # rank r's shard of the logical arrays: elements [r n, (r+1) n) of streams 1, 2, 3
     a_h = C.synth_fill(1, 1 + 10 * rank, n, 0.125, 1e-6)
     b_h = C.synth_fill(1, 2 + 10 * rank, n, 0.125, 1e-6)
     x_h = C.synth_fill(2, 3 + 10 * rank, n, 0.125, 1e-6)
@@ -202,14 +207,21 @@ def main():
     dres = torch.zeros(1, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
     step_bytes = 8.0 * n + 8.0 * n
+    sharded_dot = [0.0]
 
     def step(ev=None):
         if ev is not None:
             ev[0].record(stream)
-        C.dot(a, b, init=0.0, out=dres)
+        if world == 1:
+            C.dot(a, b, init=0.0, out=dres)
+        else:
+            sharded_dot[0] = SH.sharded_dot(a, b, 0.0)
         if ev is not None:
             ev[1].record(stream)
-        C.scan(x, True, "sum", None, out=y)
+        if world == 1:
+            C.scan(x, True, "sum", None, out=y)
+        else:
+            y.copy_(SH.sharded_scan(x, True, "sum", None))
         if ev is not None:
             ev[2].record(stream)
 
@@ -233,9 +245,6 @@ def main():
     scan_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
     clocks = clk.summary()
 
-    # parity of the timed results (one check, outside the timed region)
-    from_dot = dres.item()
-
     value = step_bytes * args.steps * world / (ms / 1e3) / 1e9
     scan_cfg = C.lib().b2p_auto_config(C.PRIM_SCAN, C.F32, n, 0, 0.0)
     dot_cfg = C.lib().b2p_auto_config(C.PRIM_DOT, C.F32, n, 0, 0.0)
@@ -251,34 +260,43 @@ def main():
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic[0] if traffic else None,
                 "algorithmic_bytes": dom_bytes}
+    if world > 1:
+        roofline["note"] = "scan time includes the shard reduce and the exchange"
 
+    config = workload_config(args.log2n, world)
+    config.update(scan_config=scan_cfg, dot_config=dot_cfg)
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"fp32 dot(a,b) 2^{args.log2n} + fp32 inclusive_scan 2^{args.log2n}",
-                   "elements": n, "step_bytes": step_bytes,
-                   "scan_config": scan_cfg, "dot_config": dot_cfg,
-                   "l2": "inputs (3 GiB) larger than the 126 MB L2; no flush",
-                   "parallelism": f"replicas x{world}"},
+        "config": config,
         "roofline": roofline,
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (2 if world == 1 else 3) * args.steps,
         "clocks": clocks,
         "per_kernel_ms": {"dot": round(dot_ms, 4), "scan": round(scan_ms, 4)},
-        "dot_result": from_dot,
-        "precision": measure_precision(torch, a, b, x, y, dres),
+        "precision": measure_precision(torch, a, b, x, y, dres if world == 1 else None),
     }
 
     if rank == 0 and world == 1:
         result["e2e"] = measure_e2e(C, torch, a_h, b_h, x_h, args)
         if not args.no_cpu:
-            result["cpu_baseline"] = cpu_baseline(a_h, b_h, x_h)
+            result["cpu_baseline"] = cpu_baseline(args.log2n)
         if not args.no_ops:
-            result["ops"] = measure_ops(C, torch, np, peak, args.ops_log2n, args.ops_reps)
+            ops = measure_ops(C, torch, np, peak, args.ops_log2n, args.ops_reps)
+            print(json.dumps({"ops_summary": ops}), flush=True)
+            result["ops"] = {k: [v["GB/s"], v["frac_hbm"], v.get("b2b_frac_hbm")] for k, v in ops.items()}
+            result["ops_columns"] = ["GB/s single launch", "frac of measured HBM", "frac back-to-back"]
             if args.ops_log2n == 28:
-                result["segmented"] = measure_segmented(C, torch, np, peak)
-                result["selector"] = measure_selector_stream(selector_state)
+                seg = measure_segmented(C, torch, np, peak)
+                print(json.dumps({"segmented_summary": seg}), flush=True)
+                result["segmented"] = {k: {"GB/s": v["learned"]["GB/s"], "frac": v["learned"]["frac_hbm"],
+                                           "x_plain": v["speedup_learned_vs_plain"]}
+                                       for k, v in seg.items() if isinstance(v, dict) and "learned" in v}
+                sel = measure_selector_stream(selector_state)
+                print(json.dumps({"selector_summary": sel}), flush=True)
+                result["selector"] = {k: sel[k] for k in ("learned_vs_exhaustive_table", "heuristic_vs_learned")
+                                      if k in sel}
         result["selector_state"] = selector_state["status"]
     else:
         result["e2e"] = None
@@ -336,7 +354,8 @@ def measure_segmented(C, torch, np, peak):
                 ms = _time_op(torch, lambda: C.check(L.b2p_plan_launch(plan, sh)), reps=10)
                 entry[pol] = {"config": L.b2p_plan_config(plan), "ms": round(ms, 4),
                               "batch_calls_per_s": round(1e3 / ms, 1),
-                              "GB/s": round(nbytes / (ms / 1e3) / 1e9, 1)}
+                              "GB/s": round(nbytes / (ms / 1e3) / 1e9, 1),
+                              "frac_hbm": round(nbytes / (ms / 1e3) / 1e9 / peak, 4)}
                 L.b2p_plan_destroy(plan)
             sb = L.b2p_scratch_bytes(C.PRIM_REDUCE if prim == C.PRIM_SEG_REDUCE else C.PRIM_SCAN, code,
                                      1 << 21, 0, C.AUTO)
@@ -436,45 +455,34 @@ def measure_precision(torch, a, b, x, y, dres):
     """Error of the timed step's fp32 results against float64 on the device
     (torch, outside the timed region): the dot relative and condition-normalised
     (|got - ref| / sum |a_i b_i|) errors, the scan's largest relative error."""
+    ref_s = torch.cumsum(x.double(), 0)
+    rel_s = ((y.double() - ref_s).abs() / ref_s.abs().clamp_min(1e-300)).max().item()
+    del ref_s
+    if dres is None:  # sharded: the scan of this rank's shard includes the carry
+        return {"reference": "float64 on the device (torch)", "scan_max_rel_err_local": rel_s}
     ad, bd = a.double(), b.double()
     prod = ad * bd
     ref = float(prod.sum().item())
     cond = float(prod.abs().sum().item())
     del ad, bd, prod
     got = float(dres.item())
-    ref_s = torch.cumsum(x.double(), 0)
-    rel_s = ((y.double() - ref_s).abs() / ref_s.abs().clamp_min(1e-300)).max().item()
-    del ref_s
     return {"reference": "float64 on the device (torch)",
             "dot_rel_err": abs(got - ref) / abs(ref), "dot_cond_err": abs(got - ref) / cond,
             "scan_max_rel_err": rel_s, "tolerance": 1e-6}
 
 
-def cpu_baseline(a_h, b_h, x_h):
-    """Oracle port of the OpenMP-backend evaluation order on the host cores,
-    on a bounded sample (2^26 elements, ~10 s of CPU work at most)."""
-    import numpy as np
+def cpu_baseline(log2n):
+    """The oracle's restatement of the reference's OpenMP backend on every
+    host core, on the same workload (oracle/baseline.py: the same process
+    setup as the reference arm), 5 timed steps after 1 warm-up."""
+    from oracle import baseline
 
-    from oracle import oracle as O
-
-    ns = 1 << 26
-    a, b, x = a_h[:ns], b_h[:ns], x_h[:ns]
-    threads = O.num_threads()
-    O.dot(O.F32, a, b, 0.0)
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        O.dot(O.F32, a, b, 0.0)
-        O.scan(O.F32, O.SUM, True, x)
-        reps += 1
-        if time.perf_counter() - t0 > 8.0 or reps >= 20:
-            break
-    dt = time.perf_counter() - t0
-    got = float(O.dot(O.F32, a, b, 0.0))
-    ref = float(np.dot(a.astype(np.float64), b.astype(np.float64)))
-    return {"value": round(16.0 * ns * reps / dt / 1e9, 3), "unit": "GB/s", "cores": threads,
-            "kind": "port", "dot_rel_err_vs_fp64": abs(got - ref) / abs(ref),
-            "sample": f"{reps} x (dot + inclusive_scan) over 2^26 fp32 elements, "
-                      f"OpenMP-backend evaluation order"}
+    r = baseline.run(log2n, 5, 1)
+    return {"value": round(r["value"], 3), "unit": "GB/s", "cores": r["threads"], "kind": "port",
+            "cpu_model": r["cpu_model"], "dot_rel_err_vs_fp64": r["dot_rel_err_vs_fp64"],
+            "scan_max_rel_err_vs_fp64": r["scan_max_rel_err_vs_fp64"],
+            "sample": f"the full workload: 5 steps of dot + inclusive_scan over 2^{log2n} fp32 elements, "
+                      f"OpenMP-backend evaluation order, {r['threads']} threads (OMP_PROC_BIND=close)"}
 
 
 def _time_b2b(torch, fn, reps=10, warm=3):
@@ -498,7 +506,7 @@ def _time_op(torch, fn, reps=10, warm=3, flush=None):
     ts = []
     for _ in range(reps):
         if flush is not None:
-            flush.zero_()
+            flush.sum()  # reads 512 MB: evicts L2 without leaving dirty lines to drain later
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         fn()

@@ -112,6 +112,13 @@ const char *b2p_version(void);
 /* Human-readable text for a status code. */
 const char *b2p_status_string(int status);
 
+/* Architecture the library's kernels were compiled for, as the CUDA runtime
+ * reports it for one of them on the current device (cudaFuncGetAttributes:
+ * binaryVersion 100 = sm_100a machine code, ptxVersion 0 when no PTX is
+ * embedded).  Stands in for the reference's device/backend query
+ * (sycl/device.hpp:66-69); the library has one target only. */
+int b2p_kernel_arch(int *binary_version, int *ptx_version);
+
 /* Configuration table entry c: threads per block {128,256,512,1024},
  * items per thread {4,8,16,32}, grid mode {0: one tile per block,
  * 1: persistent at full occupancy, 2: persistent at half occupancy}.
@@ -165,12 +172,18 @@ int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out,
  * cudaMalloc, cudaFree or other allocating routine; its scratch is a
  * B2P_STATIC_SCRATCH_BYTES array inside the library, which every GPU that
  * loads the library keeps until the process exits.
- *  - The first call on each device looks up that array's device address
- *    (cudaGetSymbolAddress, with the device current); make that first call
- *    before any stream capture.
+ *  - Every call looks up that array's device address (cudaGetSymbolAddress,
+ *    with the device current), so an address from an earlier context is
+ *    never used.  The first call on each device, and the first after its
+ *    context was rebuilt (cudaDeviceReset), also loads the library's module
+ *    and every reduce kernel this entry point can launch -- a driver-side
+ *    allocation.  Make that first call at start-up, before any stream
+ *    capture and outside any allocator callback; later calls load nothing.
  *  - All calls on a device share the one array: calls that can overlap on
  *    the GPU (different streams without ordering) race and must not be
- *    issued.  Each call clears the array's counters before its launch.
+ *    issued.  Each call clears the array's counters before its launch,
+ *    after its arguments were checked (a rejected call leaves the array as
+ *    it was).
  *  - n > B2P_STATIC_MAX_ELEMS returns B2P_ERR_INVALID_ARG; a call whose
  *    scratch need exceeds the array returns B2P_ERR_SCRATCH. */
 int b2p_reduce_static(int dtype, int op, const void *in, size_t n, void *out,

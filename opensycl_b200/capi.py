@@ -72,6 +72,7 @@ def _declare(L):
     sig = {
         "b2p_version": ([], ctypes.c_char_p),
         "b2p_status_string": ([i], ctypes.c_char_p),
+        "b2p_kernel_arch": ([ip, ip], i),
         "b2p_config_describe": ([i, ip, ip, ip], i),
         "b2p_config_valid": ([i, i, i], i),
         "b2p_scratch_bytes": ([i, i, sz, i64, i], sz),

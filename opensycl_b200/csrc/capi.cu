@@ -155,6 +155,15 @@ bool config_valid(int prim, int dtype, int config) {
   }
 }
 
+int validate_reduce(int dtype, int op, const void *in, size_t n, const void *out) {
+  if (!valid_dtype(dtype) || !valid_op(dtype, op)) return B2P_ERR_INVALID_ARG;
+  if (n == 0) return B2P_OK;
+  int rc = check_device();
+  if (rc) return rc;
+  if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, acc_size(dtype)))) return rc;
+  return B2P_OK;
+}
+
 static int resolve(int prim, int dtype, size_t n, int64_t nseg, int config) {
   if (config == B2P_CONFIG_AUTO) return b2p_auto_config(prim, dtype, n, nseg, 0.0);
   return config;
@@ -223,11 +232,8 @@ int b2p_scratch_init(void *scratch, size_t bytes, b2p_stream stream) {
 
 int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
                void *scratch, size_t scratch_bytes, int config, b2p_stream stream) {
-  if (!valid_dtype(dtype) || !valid_op(dtype, op)) return B2P_ERR_INVALID_ARG;
-  if (n == 0) return B2P_OK;
-  int rc = check_device();
-  if (rc) return rc;
-  if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, acc_size(dtype)))) return rc;
+  int rc = validate_reduce(dtype, op, in, n, out);
+  if (rc || n == 0) return rc;
   if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_REDUCE, dtype, n, 0, config);
   if (!config_valid(B2P_PRIM_REDUCE, dtype, config)) return B2P_ERR_INVALID_ARG;

@@ -40,6 +40,12 @@ long long debug_stall_tile();
 int cuda_status(cudaError_t e);
 
 // Reduce / dot.  b == nullptr: reduce; otherwise dot.
+// Argument, device and pointer checks of b2p_reduce (B2P_OK when n == 0).
+int validate_reduce(int dtype, int op, const void *in, size_t n, const void *out);
+// Loads every reduce kernel instantiation b2p_reduce can launch for a plain
+// reduce (no dot) on the current device, so that later launches load no
+// module (cudaFuncGetAttributes on each).
+int preload_reduce_kernels();
 size_t reduce_scratch_bytes(int dtype, size_t n, const void *a, const void *b);
 int launch_reduce(int dtype, int op, const void *a, const void *b, size_t n, void *out,
                   const void *init, void *scratch, size_t scratch_bytes, int config,

@@ -325,7 +325,40 @@ int dispatch_op(int op, const void *a, const void *b, size_t n, void *out, const
   }
 }
 
+template <int DT, int OP>
+int preload_one() {
+  cudaFuncAttributes fa;
+  cudaError_t e =
+      cudaFuncGetAttributes(&fa, (const void *)reduce_kernel<typename PolicyOf<DT, OP>::type, false, true>);
+  return cuda_status(e);
+}
+
+template <int DT>
+int preload_dtype() {
+  int rc = preload_one<DT, B2P_SUM>();
+  if (!rc) rc = preload_one<DT, B2P_PROD>();
+  if (!rc) rc = preload_one<DT, B2P_MIN>();
+  if (!rc) rc = preload_one<DT, B2P_MAX>();
+  if constexpr (DT != B2P_F32 && DT != B2P_BF16 && DT != B2P_F64) {
+    if (!rc) rc = preload_one<DT, B2P_AND>();
+    if (!rc) rc = preload_one<DT, B2P_OR>();
+    if (!rc) rc = preload_one<DT, B2P_XOR>();
+  }
+  return rc;
+}
+
 }  // namespace
+
+int preload_reduce_kernels() {
+  int rc = preload_dtype<B2P_I32>();
+  if (!rc) rc = preload_dtype<B2P_I64>();
+  if (!rc) rc = preload_dtype<B2P_U32>();
+  if (!rc) rc = preload_dtype<B2P_U64>();
+  if (!rc) rc = preload_dtype<B2P_F32>();
+  if (!rc) rc = preload_dtype<B2P_BF16>();
+  if (!rc) rc = preload_dtype<B2P_F64>();
+  return rc;
+}
 
 size_t reduce_scratch_bytes(int dtype, size_t n, const void *a, const void *b) {
   size_t es = dtype_size(dtype);
@@ -355,3 +388,16 @@ int launch_reduce(int dtype, int op, const void *a, const void *b, size_t n, voi
 }
 
 }  // namespace b2p
+
+extern "C" int b2p_kernel_arch(int *binary_version, int *ptx_version) {
+  using P = b2p::PolicyOf<B2P_I32, B2P_SUM>::type;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)b2p::reduce_kernel<P, false, true>);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return B2P_ERR_CUDA;
+  }
+  if (binary_version) *binary_version = fa.binaryVersion;
+  if (ptx_version) *ptx_version = fa.ptxVersion;
+  return B2P_OK;
+}

@@ -187,6 +187,8 @@ def sharded_scan(x, inclusive=True, op="sum", init=None, group=None, ops: LocalO
     ops = ops or LocalOps()
     g = Group(group)
     code = ops.code(x)
+    if g.size == 1:  # nothing to exchange: no shard total is needed
+        return ops.scan(x, inclusive, op, init if (init is not None or inclusive) else identity(code, op))
     tot = ops.reduce(x, op, identity(code, op)) if ops.numel(x) else identity(code, op)
     totals = [_from_bits(code, int(v)) for v in g.all_gather_i64([_to_bits(code, tot)])[:, 0]]
     if inclusive and init is None:

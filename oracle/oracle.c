@@ -83,10 +83,33 @@ void orc_set_num_threads(int n) {
  * path with initialization flags (reduction_engine / wi_reducer.hpp:59-70).
  * ---------------------------------------------------------------------- */
 
+/* Thread count and id inside a parallel region (1 and 0 without OpenMP). */
+#define DEFINE_THREAD_IDS(NAME)                                                \
+  static inline void NAME##_thread_ids(size_t *nt, size_t *tid) {              \
+    *nt = (size_t)omp_get_num_threads_or_1();                                  \
+    *tid = (size_t)omp_get_thread_num_or_0();                                  \
+  }
+
+static inline int omp_get_num_threads_or_1(void) {
+#ifdef _OPENMP
+  return omp_get_num_threads();
+#else
+  return 1;
+#endif
+}
+static inline int omp_get_thread_num_or_0(void) {
+#ifdef _OPENMP
+  return omp_get_thread_num();
+#else
+  return 0;
+#endif
+}
+
 /* Generic reduce generator.  T = accumulation type, IN = input element type,
  * CVT converts one input element to T. */
 #define DEFINE_REDUCE(NAME, T, IN, CVT, COMBINE, IDENT_SUM, IDENT_PROD,        \
                       IDENT_MIN, IDENT_MAX)                                    \
+  DEFINE_THREAD_IDS(NAME)                                                      \
   static T NAME##_comb(int op, T a, T b) { return COMBINE(op, a, b); }         \
   static int NAME##_ident(int op, T *id) {                                     \
     switch (op) {                                                              \
@@ -186,48 +209,66 @@ void orc_set_num_threads(int n) {
   }                                                                            \
   /* OMP-backend scan: algorithms/scan/scan.hpp:26-32 (WG 1024 on OMP),       \
    * decoupled_lookback_scan.hpp:137-177 (one leader scans the 16*1024        \
-   * tile sequentially), :219-257 (look-back; in serial order the            \
-   * predecessor's inclusive prefix is always available), :259-277           \
-   * (exclusive = shifted inclusive with x[-1] := init; out-of-range         \
-   * generator ids clamp to n-1, scan.hpp:58-66). */                          \
+   * tile sequentially into local memory, finds the tile's exclusive prefix,  \
+   * then writes op(prefix, local[i]) -- one write per element), :219-257     \
+   * (look-back; here the predecessor's inclusive prefix, so the carries     \
+   * form the serial chain prefix[g] = op(prefix[g-1], agg[g]) whatever the   \
+   * timing), :259-277 (exclusive = shifted inclusive with x[-1] := init;     \
+   * out-of-range generator ids clamp to n-1, scan.hpp:58-66).  Threads take  \
+   * tiles round-robin and each waits only for its predecessor's prefix,      \
+   * which is published as soon as that tile's local scan is done. */         \
   static void NAME##_omp_scan(int op, int inclusive, const IN *x, T *y,       \
                               size_t n, const T *init) {                       \
     const size_t TILE = 16 * 1024;                                             \
     size_t ntiles = ((n + 15) / 16 + 1023) / 1024;                             \
-    T *agg = (T *)malloc(sizeof(T) * ntiles);                                  \
-    _Pragma("omp parallel for schedule(static)")                               \
-    for (size_t g = 0; g < ntiles; ++g) {                                      \
-      T cur;                                                                   \
-      memset(&cur, 0, sizeof(T));                                              \
-      for (size_t i = 0; i < TILE; ++i) {                                      \
-        size_t gid = g * TILE + i;                                             \
-        T e;                                                                   \
-        if (inclusive) {                                                       \
-          size_t src = gid < n ? gid : n - 1;                                  \
-          e = CVT(x[src]);                                                     \
-          if (init && gid == 0) e = NAME##_comb(op, *init, e);                 \
-        } else {                                                               \
-          if (gid == 0) e = *init;                                             \
-          else {                                                               \
-            size_t src = gid - 1 < n ? gid - 1 : n - 1;                        \
+    T *pre = (T *)malloc(sizeof(T) * ntiles);                                  \
+    int *ready = (int *)calloc(ntiles, sizeof(int));                           \
+    _Pragma("omp parallel")                                                    \
+    {                                                                          \
+      size_t nt = 1, tid = 0;                                                  \
+      NAME##_thread_ids(&nt, &tid);                                            \
+      T *loc = (T *)malloc(sizeof(T) * TILE);                                  \
+      for (size_t g = tid; g < ntiles; g += nt) {                              \
+        T cur;                                                                 \
+        memset(&cur, 0, sizeof(T));                                            \
+        for (size_t i = 0; i < TILE; ++i) {                                    \
+          size_t gid = g * TILE + i;                                           \
+          T e;                                                                 \
+          if (inclusive) {                                                     \
+            size_t src = gid < n ? gid : n - 1;                                \
             e = CVT(x[src]);                                                   \
+            if (init && gid == 0) e = NAME##_comb(op, *init, e);               \
+          } else {                                                             \
+            if (gid == 0) e = *init;                                           \
+            else {                                                             \
+              size_t src = gid - 1 < n ? gid - 1 : n - 1;                      \
+              e = CVT(x[src]);                                                 \
+            }                                                                  \
           }                                                                    \
+          cur = (i == 0) ? e : NAME##_comb(op, cur, e);                        \
+          loc[i] = cur;                                                        \
         }                                                                      \
-        cur = (i == 0) ? e : NAME##_comb(op, cur, e);                          \
-        if (gid < n) y[gid] = cur;                                             \
+        if (g == 0) {                                                          \
+          pre[0] = cur;                                                        \
+        } else {                                                               \
+          while (!__atomic_load_n(&ready[g - 1], __ATOMIC_ACQUIRE))            \
+            __builtin_ia32_pause();                                            \
+          pre[g] = NAME##_comb(op, pre[g - 1], cur);                           \
+        }                                                                      \
+        __atomic_store_n(&ready[g], 1, __ATOMIC_RELEASE);                      \
+        size_t end = (g + 1) * TILE < n ? (g + 1) * TILE : n;                  \
+        if (g == 0) {                                                          \
+          for (size_t gid = 0; gid < end; ++gid) y[gid] = loc[gid];            \
+        } else {                                                               \
+          T p = pre[g - 1];                                                    \
+          for (size_t gid = g * TILE; gid < end; ++gid)                        \
+            y[gid] = NAME##_comb(op, p, loc[gid - g * TILE]);                  \
+        }                                                                      \
       }                                                                        \
-      agg[g] = cur;                                                            \
+      free(loc);                                                               \
     }                                                                          \
-    /* serial prefix chain: inclusive_prefix[g] = op(prefix[g-1], agg[g]) */   \
-    for (size_t g = 1; g < ntiles; ++g) agg[g] = NAME##_comb(op, agg[g - 1], agg[g]); \
-    _Pragma("omp parallel for schedule(static)")                               \
-    for (size_t g = 1; g < ntiles; ++g) {                                      \
-      T pre = agg[g - 1];                                                      \
-      size_t end = (g + 1) * TILE < n ? (g + 1) * TILE : n;                    \
-      for (size_t gid = g * TILE; gid < end; ++gid)                            \
-        y[gid] = NAME##_comb(op, pre, y[gid]);                                 \
-    }                                                                          \
-    free(agg);                                                                 \
+    free(pre);                                                                 \
+    free(ready);                                                               \
   }
 
 #define COMB_INT(U) (U)
@@ -583,4 +624,112 @@ int orc_fp64_segmented_sum(int dtype, const void *x, const int64_t *offs,
     out[s] = t.hi + t.lo;
   }
   return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Seeded synthetic inputs, bit-identical to the library's b2p_synth_fill
+ * (include/b2p.h): SplitMix64 finaliser over (seed, index, stream), uniform
+ * on (0, 1] from the top 53 bits, Box-Muller in double rounded once, bf16 by
+ * round-to-nearest-even, truncated Zipf keys by an inverse-CDF table.  The
+ * CPU baseline and the reference arm of the benchmark generate their inputs
+ * with this, so that they load nothing but this library;
+ * tests/test_oracle_golden.py checks that both generators agree.
+ * ---------------------------------------------------------------------- */
+static inline uint64_t syn_mix(uint64_t seed, uint64_t i, uint64_t stream) {
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + (i + 1) * 0xD1B54A32D192ED03ull +
+               (stream + 1) * 0x8CB92BA72F3D8DD7ull;
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static inline double syn_unif(uint64_t seed, uint64_t i, uint64_t stream) {
+  return (double)((syn_mix(seed, i, stream) >> 11) + 1) * 0x1.0p-53;
+}
+static inline double syn_normal(uint64_t seed, uint64_t i, uint64_t s0) {
+  const double u1 = syn_unif(seed, i, s0), u2 = syn_unif(seed, i, s0 + 1);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+static inline float syn_mixed_normal(uint64_t seed, uint64_t i, double frac, double scale) {
+  if (frac > 0.0 && syn_unif(seed, i, 3) <= frac) return (float)(scale * syn_normal(seed, i, 4));
+  return (float)syn_normal(seed, i, 1);
+}
+static inline uint16_t syn_bf16_rne(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+/* kinds as b2p_synth_fill: 0 int32 U[a,b], 1 fp32 N(0,1) with a fraction a
+ * scaled by b, 2 |kind 1|, 3 uint32, 4 uint8 Zipf(a), 5 int64 U[a,b],
+ * 6 / 7 bf16 bits of kinds 1 / 2.  Returns 0, or -1 for a bad kind. */
+int orc_synth_fill(int kind, uint64_t seed, size_t n, double a, double b, void *out) {
+  const long long N = (long long)n;
+  switch (kind) {
+  case 0:
+  case 5: {
+    const long long lo = (long long)a, span = (long long)b - lo + 1;
+    if (span <= 0) return -1;
+    _Pragma("omp parallel for schedule(static)")
+    for (long long i = 0; i < N; ++i) {
+      const long long v = lo + (long long)(syn_mix(seed, (uint64_t)i, 0) % (uint64_t)span);
+      if (kind == 0) ((int32_t *)out)[i] = (int32_t)v;
+      else ((int64_t *)out)[i] = (int64_t)v;
+    }
+    return 0;
+  }
+  case 1:
+  case 2: {
+    float *o = (float *)out;
+    _Pragma("omp parallel for schedule(static)")
+    for (long long i = 0; i < N; ++i) {
+      float v = syn_mixed_normal(seed, (uint64_t)i, a, b);
+      o[i] = kind == 2 ? fabsf(v) : v;
+    }
+    return 0;
+  }
+  case 3: {
+    uint32_t *o = (uint32_t *)out;
+    _Pragma("omp parallel for schedule(static)")
+    for (long long i = 0; i < N; ++i) o[i] = (uint32_t)(syn_mix(seed, (uint64_t)i, 0) >> 32);
+    return 0;
+  }
+  case 4: {
+    const double s = a > 0 ? a : 1.2;
+    double cdf[256], acc = 0.0;
+    for (int r = 1; r <= 256; ++r) {
+      acc += pow((double)r, -s);
+      cdf[r - 1] = acc;
+    }
+    for (int r = 0; r < 256; ++r) cdf[r] /= acc;
+    cdf[255] = 1.0;
+    uint8_t *o = (uint8_t *)out;
+    _Pragma("omp parallel for schedule(static)")
+    for (long long i = 0; i < N; ++i) {
+      const double u = syn_unif(seed, (uint64_t)i, 0);
+      int lo = 0, hi = 256; /* first k with cdf[k] >= u */
+      while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (cdf[mid] < u) lo = mid + 1;
+        else hi = mid;
+      }
+      o[i] = (uint8_t)(lo > 255 ? 255 : lo);
+    }
+    return 0;
+  }
+  case 6:
+  case 7: {
+    uint16_t *o = (uint16_t *)out;
+    _Pragma("omp parallel for schedule(static)")
+    for (long long i = 0; i < N; ++i) {
+      float v = syn_mixed_normal(seed, (uint64_t)i, a, b);
+      o[i] = syn_bf16_rne(kind == 7 ? fabsf(v) : v);
+    }
+    return 0;
+  }
+  default:
+    return -1;
+  }
 }

@@ -53,11 +53,12 @@ def lib():
         L.orc_fp64_sum.argtypes = [i, vp, vp, sz, ctypes.c_double, vp, vp, vp]
         L.orc_fp64_scan.argtypes = [i, i, vp, sz, ctypes.c_double, vp]
         L.orc_fp64_segmented_sum.argtypes = [i, vp, vp, ctypes.c_int64, vp]
+        L.orc_synth_fill.argtypes = [i, ctypes.c_uint64, sz, ctypes.c_double, ctypes.c_double, vp]
         L.orc_set_num_threads.argtypes = [i]
         L.orc_num_threads.restype = i
         for f in ("orc_reduce", "orc_dot", "orc_scan", "orc_copy_if_u32", "orc_histogram_u8",
                   "orc_segmented_reduce", "orc_segmented_scan", "orc_fp64_sum",
-                  "orc_fp64_scan", "orc_fp64_segmented_sum"):
+                  "orc_fp64_scan", "orc_fp64_segmented_sum", "orc_synth_fill"):
             getattr(L, f).restype = i
         _lib = L
     return _lib
@@ -77,6 +78,19 @@ def set_threads(n: int) -> None:
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+SYNTH_NP = {0: np.int32, 1: np.float32, 2: np.float32, 3: np.uint32, 4: np.uint8, 5: np.int64,
+            6: np.uint16, 7: np.uint16}
+
+
+def synth_fill(kind, seed, n, a=0.0, b=0.0, out=None):
+    """Seeded synthetic inputs, the same bits as the library's b2p_synth_fill."""
+    if out is None:
+        out = np.empty(n, dtype=SYNTH_NP[kind])
+    rc = lib().orc_synth_fill(int(kind), int(seed), int(n), float(a), float(b), _p(out))
+    assert rc == 0
+    return out
 
 
 def reduce(dtype, op, x, init, out_init=None):
@@ -100,10 +114,11 @@ def dot(dtype, a, b, init=0.0):
     return out[0]
 
 
-def scan(dtype, op, inclusive, x, init=None):
+def scan(dtype, op, inclusive, x, init=None, out=None):
     x = np.ascontiguousarray(x, dtype=NP_OF[dtype])
     acc = ACC_OF[dtype]
-    y = np.zeros(x.size, dtype=acc)
+    y = np.zeros(x.size, dtype=acc) if out is None else out
+    assert y.dtype == acc and y.size == x.size and y.flags.c_contiguous
     ini = _scalar(init, acc) if init is not None else None
     rc = lib().orc_scan(dtype, op, int(bool(inclusive)), _p(x), _p(y), x.size, _p(ini))
     assert rc == 0

@@ -523,6 +523,84 @@ static void test_stdpar() {
   CHECK(!b2p_stdpar::offload_history().empty(), "stdpar offload history recorded");
 }
 
+// ----------------------------------------------- workload configurations
+// Config 1: 2^24 int32 U[-1000, 1000] (seed 0) through the entry points it
+// names -- sycl::reduction in parallel_for, std::reduce and
+// std::inclusive_scan on the stdpar policy -- bit-exact against a host sum /
+// scan.  Config 3: hipsycl::algorithms::copy_if with a lambda predicate
+// (x & 7) < 3 on 2^28 uint32 (seed 4), bit-exact and order-preserving.
+// Config 2's fp32 values (seed 1) through sycl::reduction: within 1e-6 of a
+// float64 host sum.
+
+static void test_workload_configs(sycl::queue &q) {
+  alg::util::allocation_cache cache{alg::util::allocation_type::device};
+  {
+    const size_t n = 1ul << 24;
+    std::vector<int32_t> h(n);
+    CHECK(b2p_synth_fill(0, 0, n, -1000, 1000, h.data()) == B2P_OK, "synth config 1");
+    uint32_t wrap = 0;
+    for (int32_t v : h) wrap += (uint32_t)v;
+    const int32_t ref = (int32_t)wrap;
+    int32_t *d = to_dev(q, h);
+    int32_t *sum = sycl::malloc_shared<int32_t>(1, q);
+    *sum = 0;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<int32_t>{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; })
+        .wait();
+    CHECK(*sum == ref, "config 1 sycl::reduction 2^24 got %d want %d", *sum, ref);
+    const auto &pol = b2p_stdpar::par_unseq;
+    const int32_t sr = std::reduce(pol, h.begin(), h.end(), (int32_t)0);
+    CHECK(sr == ref, "config 1 std::reduce 2^24 got %d want %d", sr, ref);
+    std::vector<int32_t> sc(n), scr(n);
+    std::inclusive_scan(pol, h.begin(), h.end(), sc.begin());
+    uint32_t run = 0;
+    for (size_t i = 0; i < n; ++i) scr[i] = (int32_t)(run += (uint32_t)h[i]);
+    CHECK(sc == scr, "config 1 std::inclusive_scan 2^24");
+    sycl::free(sum, q);
+    sycl::free(d, q);
+  }
+  {
+    const size_t n = 1ul << 28;
+    std::vector<float> h(n);
+    CHECK(b2p_synth_fill(1, 1, n, 0.125, 1e-6, h.data()) == B2P_OK, "synth config 2");
+    double ref = 0.0;
+    for (float v : h) ref += (double)v;
+    float *d = to_dev(q, h);
+    float *sum = sycl::malloc_shared<float>(1, q);
+    *sum = 0.f;
+    q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<float>{}),
+                   [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; })
+        .wait();
+    CHECK(std::fabs((double)*sum - ref) <= 1e-6 * std::fabs(ref), "fp32 sycl::reduction 2^28 got %.9g want %.9g",
+          (double)*sum, ref);
+    sycl::free(sum, q);
+    sycl::free(d, q);
+  }
+  {
+    const size_t n = 1ul << 28;
+    std::vector<uint32_t> h(n);
+    CHECK(b2p_synth_fill(3, 4, n, 0, 0, h.data()) == B2P_OK, "synth config 3");
+    std::vector<uint32_t> ref;
+    ref.reserve(n / 2);
+    for (uint32_t v : h)
+      if ((v & 7u) < 3u) ref.push_back(v);
+    uint32_t *d = to_dev(q, h);
+    uint32_t *out = sycl::malloc_device<uint32_t>(n, q);
+    size_t *cnt = sycl::malloc_shared<size_t>(1, q);
+    *cnt = 0;
+    {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      alg::copy_if(q, g, d, d + n, out, [] __host__ __device__(uint32_t v) { return (v & 7u) < 3u; }, cnt).wait();
+    }
+    CHECK(*cnt == ref.size(), "config 3 lambda copy_if count %zu want %zu", *cnt, ref.size());
+    std::vector<uint32_t> got = from_dev(q, out, ref.size());
+    CHECK(got == ref, "config 3 lambda copy_if values");
+    sycl::free(cnt, q);
+    sycl::free(out, q);
+    sycl::free(d, q);
+  }
+}
+
 int main() {
   try {
     sycl::queue q;
@@ -531,6 +609,7 @@ int main() {
     test_group_functions(q);
     test_atomics(q);
     test_stdpar();
+    test_workload_configs(q);
   } catch (const std::exception &e) {
     std::printf("FAIL exception: %s\n", e.what());
     return 2;

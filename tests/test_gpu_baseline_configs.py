@@ -67,3 +67,68 @@ def test_config3_exclusive_scan_copy_if_histogram(dev):
     k = C.synth_fill(4, 5, N28, 1.2)
     bins = C.histogram_u8(torch.from_numpy(k).cuda())
     assert np.array_equal(bins.cpu().numpy().astype(np.int64), O.histogram_u8(k).astype(np.int64))
+
+
+def _plan_run(prim, code, x, out, od, nseg, total):
+    import ctypes
+    L = C.lib()
+    plan = ctypes.c_void_p()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    C.check(L.b2p_plan_segmented(ctypes.byref(plan), prim, code, C.SUM, x.data_ptr(), out.data_ptr(),
+                                 od.data_ptr(), nseg, total, C.AUTO, s), "plan")
+    try:
+        for _ in range(2):  # a replayed graph gives the same result
+            out.fill_(7)
+            C.check(L.b2p_plan_launch(plan, s), "launch")
+            torch.cuda.synchronize()
+    finally:
+        L.b2p_plan_destroy(plan)
+    return out.cpu().numpy()
+
+
+def test_config4_segmented_full_shape(dev):
+    """10,000 segments with lengths log-uniform in [1, 2^20] scaled to 2^28
+    elements in total (seed 6), fp32 N(0,1) (seed 7) and int64
+    U[-2^20, 2^20] (seed 8): per-segment sum and inclusive scan through the
+    CUDA-graph plan, as the benchmark runs them.  int64 bit-exact against the
+    oracle; fp32 against float64 within 1e-6 relative, plus a condition term
+    for segments and prefixes whose sum cancels (values of both signs):
+    reduce 1e-12 * sum|x|, scan 2^-22 * prefix sum|x| (one fp32 rounding of
+    the thread-local running value)."""
+    nseg = 10000
+    offs = C.synth_segments(6, nseg, 20.0, N28)
+    total = int(offs[-1])
+    assert total > 0.99 * N28 and np.diff(offs).min() >= 1
+    od = torch.from_numpy(offs).cuda()
+    # int64
+    x = C.synth_fill(5, 8, total, -(1 << 20), 1 << 20)
+    xd = torch.from_numpy(x).cuda()
+    got = _plan_run(C.PRIM_SEG_REDUCE, C.I64, xd, torch.empty(nseg, dtype=torch.int64, device="cuda"),
+                    od, nseg, total)
+    assert np.array_equal(got, O.segmented_reduce(O.I64, O.SUM, x, offs))
+    yd = torch.empty(total, dtype=torch.int64, device="cuda")
+    got = _plan_run(C.PRIM_SEG_SCAN, C.I64, xd, yd, od, nseg, total)
+    assert np.array_equal(got, O.segmented_scan(O.I64, O.SUM, True, x, offs))
+    del x, xd, yd, got
+    # fp32
+    x = C.synth_fill(1, 7, total, 0.0, 0.0)
+    xd = torch.from_numpy(x).cuda()
+    got = _plan_run(C.PRIM_SEG_REDUCE, C.F32, xd, torch.empty(nseg, dtype=torch.float32, device="cuda"),
+                    od, nseg, total).astype(np.float64)
+    ref = O.fp64_segmented_sum(O.F32, x, offs)
+    sabs = np.add.reduceat(np.abs(x).astype(np.float64), offs[:-1])
+    assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-12 * sabs)
+    yd = torch.empty(total, dtype=torch.float32, device="cuda")
+    y = _plan_run(C.PRIM_SEG_SCAN, C.F32, xd, yd, od, nseg, total)
+    del yd, xd
+    worst = 0.0
+    for s in range(nseg):
+        a, b = int(offs[s]), int(offs[s + 1])
+        seg = x[a:b].astype(np.float64)
+        r = np.cumsum(seg)
+        cabs = np.cumsum(np.abs(seg))
+        err = np.abs(y[a:b].astype(np.float64) - r)
+        tol = 1e-6 * np.abs(r) + 2.0 ** -22 * cabs
+        assert np.all(err <= tol), (s, float(np.max(err / tol)))
+        worst = max(worst, float(np.max(err / np.maximum(cabs, 1e-300))))
+    assert worst <= 2.0 ** -22

@@ -463,3 +463,12 @@ def test_errors_are_status_codes(dev):
     assert L.b2p_reduce(C.F32, C.SUM, x.data_ptr() + 2, 10, out.data_ptr(), None, sp, sb, 0, None) == C.ERR_INVALID_PTR
     torch.cuda.synchronize()
     assert C.device_error() == C.OK
+
+
+def test_kernels_are_sm100a(dev):
+    """The kernels the CUDA runtime loads from libb2p are sm_100a machine code
+    (cudaFuncGetAttributes binaryVersion 100), with no PTX to JIT."""
+    import ctypes
+    b, p = ctypes.c_int(0), ctypes.c_int(-1)
+    C.check(C.lib().b2p_kernel_arch(ctypes.byref(b), ctypes.byref(p)), "b2p_kernel_arch")
+    assert b.value == 100, b.value

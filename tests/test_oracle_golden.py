@@ -136,3 +136,34 @@ def test_segmented_matches_per_segment_calls():
     y = O.segmented_scan(O.I64, O.SUM, True, x, offs)
     for s in range(40):
         assert (y[offs[s]:offs[s + 1]] == np.cumsum(x[offs[s]:offs[s + 1]])).all()
+
+
+def test_oracle_generator_matches_library_generator():
+    """The oracle's copy of the seeded generator (used by the CPU baseline and
+    the benchmark's reference arm) gives the library generator's bits."""
+    from opensycl_b200 import capi as C
+    for kind, seed, a, b in [(0, 0, -1000, 1000), (1, 1, 0.125, 1e-6), (2, 3, 0.125, 1e-6), (3, 4, 0, 0),
+                             (4, 5, 1.2, 0), (5, 8, -(1 << 20), 1 << 20), (6, 1, 0.125, 1e-6),
+                             (7, 3, 0.125, 1e-6)]:
+        x = O.synth_fill(kind, seed, 200003, a, b)
+        y = C.synth_fill(kind, seed, 200003, a, b)
+        assert x.dtype == y.dtype and np.array_equal(x.view(np.uint8), y.view(np.uint8)), kind
+
+
+def test_single_write_scan_tiles_and_threads():
+    """The scan writes each element once after its tile's prefix is known;
+    the result must not depend on the thread count (carries form the serial
+    chain whatever the timing), across tile boundaries and a ragged end."""
+    x = O.synth_fill(2, 3, 5 * 16384 + 77, 0.125, 1e-6)
+    xi = O.synth_fill(0, 0, 5 * 16384 + 77, -1000, 1000)
+    runs = []
+    t0 = O.num_threads()
+    for t in (1, 3, 8):
+        O.set_threads(t)
+        runs.append((O.scan(O.F32, O.SUM, True, x), O.scan(O.I32, O.SUM, False, xi, 7)))
+    O.set_threads(t0)
+    for f, i in runs[1:]:
+        assert f.tobytes() == runs[0][0].tobytes()
+        assert np.array_equal(i, runs[0][1])
+    ref = (7 + np.concatenate([[0], np.cumsum(xi.astype(np.int64))[:-1]])).astype(np.int32)
+    assert np.array_equal(runs[0][1], ref)
