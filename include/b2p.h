@@ -266,6 +266,10 @@ int b2p_device_error(void *scratch, b2p_stream stream, int clear);
  * (default 2e9).  Returns the previous value. */
 uint64_t b2p_set_wait_timeout_ns(uint64_t ns);
 
+/* The current bound (read by the header-compiled kernels of the C++ layer,
+ * which honour the same limit). */
+uint64_t b2p_wait_timeout_ns(void);
+
 /* Test hook: the scan tile with this index (-1 = none) never publishes its
  * status in the next scan/copy_if launches, so its successors' bounded waits
  * run out.  Used only by the time-out test. */

@@ -12,7 +12,7 @@
 #include <cstring>
 #include <type_traits>
 
-#include "../../include/b2p.h"
+#include "../b2p.h"
 
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
 #error "libb2p is built for sm_100a only"

@@ -86,6 +86,38 @@ __device__ __forceinline__ unsigned long long publish_value(typename P::Acc a) {
   else return P::pack(a);
 }
 
+// (flag, value) pair of the segmented operator: f = a segment head lies in
+// the span, v = the combination after the last head (of everything when
+// f == 0).  (f1, v1) + (f2, v2) = (f1 | f2, f2 ? v2 : v1 + v2).
+template <class P>
+struct SegPair {
+  typename P::Acc v;
+  int f;
+};
+
+template <class P>
+struct SegOps {
+  using Pub = SegPair<P>;
+  __device__ static Pub identity() { return Pub{P::identity(), 0}; }
+  __device__ static Pub combine(Pub a, Pub b) {
+    return Pub{b.f ? b.v : P::combine(a.v, b.v), a.f | b.f};
+  }
+};
+
+template <class P>
+__device__ __forceinline__ SegPair<P> shfl_up(SegPair<P> a, int d) {
+  a.v = shfl_up(a.v, d);
+  a.f = __shfl_up_sync(0xffffffffu, a.f, d);
+  return a;
+}
+
+template <class P>
+__device__ __forceinline__ SegPair<P> shfl_idx(SegPair<P> a, int src) {
+  a.v = shfl_idx(a.v, src);
+  a.f = __shfl_sync(0xffffffffu, a.f, src);
+  return a;
+}
+
 // copy_if predicate: (bits of v & mask) CMP rhs, compared as unsigned.
 template <class T>
 __device__ __forceinline__ bool pred_bits(T v, unsigned long long mask, int cmp,

@@ -17,6 +17,8 @@
 
 #include "common.cuh"
 
+#include <mutex>
+
 namespace b2p {
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
@@ -96,6 +98,17 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int 
       : "memory");
 }
 
+// Global -> shared untiled bulk copy of `bytes` (16-byte aligned addresses,
+// a multiple of 16 bytes); completes `bytes` on *bar.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                          unsigned long long pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 // Wait until at most N of this thread's bulk groups still read shared memory.
@@ -137,6 +150,38 @@ struct RingPos {
 // swizzle.  base must be 16-byte aligned, 1 <= rows < 2^31, 1 <= box_rows
 // <= 256.  Returns false when the driver entry point is missing or rejects
 // the description.
-bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long rows, int box_rows);
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+inline EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+inline bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn || !base || (reinterpret_cast<uintptr_t>(base) & 15) || rows < 1 || rows >= (1ull << 31) ||
+      box_rows < 1 || box_rows > 256)
+    return false;
+  const cuuint64_t dims[2] = {128, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 
 }  // namespace b2p

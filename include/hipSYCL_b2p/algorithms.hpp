@@ -26,6 +26,7 @@
 #pragma once
 
 #include "sycl.hpp"
+#include "../b2p_device/copy_if.cuh"
 
 #include <algorithm>
 #include <functional>
@@ -293,6 +294,24 @@ struct binary_gen {
   __device__ T operator()(size_t i) const { return static_cast<T>(tr(*(a + i), *(b + i))); }
 };
 
+// Units of the library reduce kernel for user transforms: value(i) =
+// transform(first[i]) or transform(a[i], b[i]), converted to T.
+template <class T, class It, class Tr>
+struct unary_source : ::b2p::ValueSource<unary_source<T, It, Tr>, T> {
+  It first;
+  Tr tr;
+  unary_source(It f, Tr t) : first(f), tr(t) {}
+  __device__ __forceinline__ T value(long long i) const { return static_cast<T>(tr(*(first + i))); }
+};
+template <class T, class It1, class It2, class Tr>
+struct binary_source : ::b2p::ValueSource<binary_source<T, It1, It2, Tr>, T> {
+  It1 a;
+  It2 b;
+  Tr tr;
+  binary_source(It1 a_, It2 b_, Tr t) : a(a_), b(b_), tr(t) {}
+  __device__ __forceinline__ T value(long long i) const { return static_cast<T>(tr(*(a + i), *(b + i))); }
+};
+
 // Tile totals (one tile of kGT elements per block).
 template <class T, class Gen, class Op>
 __global__ void __launch_bounds__(kGB) tile_reduce_kernel(size_t n, Gen gen, Op op, T *tot_v, bool *tot_h) {
@@ -398,14 +417,34 @@ __global__ void __launch_bounds__(kGB) tile_count_kernel(size_t n, It first, Pre
   if (threadIdx.x == 0) cnt[blockIdx.x] = s[0];
 }
 
-__global__ void __launch_bounds__(1) counts_scan_kernel(size_t ntiles, unsigned long long *cnt, size_t *num) {
-  unsigned long long run = 0;
-  for (size_t i = 0; i < ntiles; ++i) {
-    const unsigned long long c = cnt[i];
-    cnt[i] = run;
-    run += c;
+// Exclusive scan of the tile counts in place by one block (chunks of kGB
+// counts, a shuffle scan per warp), and the total into *num.
+template <int = 0>
+__global__ void __launch_bounds__(kGB) counts_scan_kernel(size_t ntiles, unsigned long long *cnt, size_t *num) {
+  __shared__ unsigned long long s_warp[kGB / 32];
+  __shared__ unsigned long long s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (size_t b0 = 0; b0 < ntiles; b0 += kGB) {
+    const size_t i = b0 + threadIdx.x;
+    const unsigned long long c = i < ntiles ? cnt[i] : 0ull;
+    unsigned long long incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long o = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += o;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    unsigned long long before = s_carry;
+    for (int w = 0; w < warp; ++w) before += s_warp[w];
+    if (i < ntiles) cnt[i] = before + incl - c;
+    __syncthreads();
+    if (threadIdx.x == kGB - 1) s_carry = before + incl;
+    __syncthreads();
   }
-  if (num) *num = (size_t)run;
+  if (threadIdx.x == 0 && num) *num = (size_t)s_carry;
 }
 
 template <class It, class OutIt, class Pred>
@@ -458,6 +497,20 @@ bs::event generic_scan(bs::queue &q, util::allocation_group &scratch, size_t n, 
                                                              nullptr, nullptr);
   tile_scan_kernel<T, Gen, Op, OutIt, INCL><<<(unsigned)ntiles, kGB, 0, q.cuda_stream()>>>(n, gen, op, v, h, out);
   bs::detail::check_cuda(cudaGetLastError(), "generic scan");
+  return q.record();
+}
+
+// The library reduce kernel over a generated sequence (a user transform of
+// contiguous device inputs, a standard operator on int32/uint32/int64/uint64/
+// float/double): *out = op(init, r).
+template <class T, class Op, class Src>
+bs::event library_reduce(bs::queue &q, util::allocation_group &scratch, size_t n, const Src &src, T *out,
+                         T init) {
+  using P = bs::detail::library_policy<T, Op>;
+  const size_t bytes = ::b2p::reduce_gen_scratch_bytes(n);
+  void *s = scratch.obtain_scratch(bytes, q.cuda_stream());
+  bs::detail::device_guard g(q.get_device().cuda_ordinal());
+  bs::detail::check_b2p(::b2p::launch_reduce_gen<P>(src, n, out, &init, s, bytes, q.cuda_stream()), "transform_reduce");
   return q.record();
 }
 
@@ -521,6 +574,10 @@ b2p_sycl::event transform_reduce(b2p_sycl::queue &q, util::allocation_group &scr
   detail::require_device(first1, "transform_reduce");
   detail::require_device(first2, "transform_reduce");
   detail::require_device(out, "transform_reduce");
+  if constexpr (b2p_sycl::detail::library_reduction<T, BinaryReductionOp>()) {
+    detail::binary_source<T, ForwardIt1, ForwardIt2, BinaryTransformOp> src(first1, first2, transform);
+    return detail::library_reduce<T, BinaryReductionOp>(q, scratch, n, src, out, init);
+  }
   detail::binary_gen<T, ForwardIt1, ForwardIt2, BinaryTransformOp> gen{first1, first2, transform};
   return detail::generic_reduce(q, scratch, n, gen, out, init, reduce);
 }
@@ -549,6 +606,10 @@ b2p_sycl::event transform_reduce(b2p_sycl::queue &q, util::allocation_group &scr
   }
   detail::require_device(first, "transform_reduce");
   detail::require_device(out, "transform_reduce");
+  if constexpr (b2p_sycl::detail::library_reduction<T, BinaryReductionOp>()) {
+    detail::unary_source<T, ForwardIt, UnaryTransformOp> src(first, transform);
+    return detail::library_reduce<T, BinaryReductionOp>(q, scratch, n, src, out, init);
+  }
   detail::unary_gen<T, ForwardIt, UnaryTransformOp> gen{first, transform};
   return detail::generic_reduce(q, scratch, n, gen, out, init, reduce);
 }
@@ -708,11 +769,31 @@ b2p_sycl::event copy_if(b2p_sycl::queue &q, util::allocation_group &scratch, For
   detail::require_device(first, "copy_if");
   detail::require_device(d_first, "copy_if");
   if (num_elements_copied) detail::require_device(num_elements_copied, "copy_if count");
+  // Any predicate on contiguous 4- or 8-byte elements: the library's
+  // TMEM-staged copy_if kernel compiled with the predicate (16-byte aligned
+  // input of at least one 8192-element tile; the generic kernels otherwise).
+  if constexpr (detail::is_ptr<ForwardIt1> && detail::is_ptr<ForwardIt2> &&
+                (sizeof(V) == 4 || sizeof(V) == 8) && std::is_trivially_copyable_v<V> &&
+                std::is_same_v<std::remove_cv_t<detail::value_t<ForwardIt2>>, V>) {
+    constexpr int items = sizeof(V) == 4 ? 32 : 16;
+    if (n >= (size_t)256 * items && (reinterpret_cast<uintptr_t>(&*first) & 15) == 0) {
+      const int pdt = sizeof(V) == 4 ? B2P_U32 : B2P_U64;
+      const size_t bytes = b2p_scratch_bytes(B2P_PRIM_COPY_IF, pdt, n, 0, B2P_CONFIG_AUTO);
+      void *s = scratch.obtain_scratch(bytes, q.cuda_stream());
+      b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+      const int dev = q.get_device().cuda_ordinal();
+      const int rc = ::b2p::launch_copy_if_pred<V>(
+          &*first, &*d_first, n, pred, reinterpret_cast<unsigned long long *>(num_elements_copied), s, 256, items,
+          ::b2p::device_sm_count(dev), b2p_wait_timeout_ns(), -1, q.cuda_stream());
+      if (rc == B2P_OK) return q.record();
+      if (rc != B2P_ERR_UNSUPPORTED) b2p_sycl::detail::check_b2p(rc, "copy_if");
+    }
+  }
   const size_t ntiles = (n + detail::kGT - 1) / detail::kGT;
   unsigned long long *cnt = scratch.obtain<unsigned long long>(ntiles);
   b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
   detail::tile_count_kernel<<<(unsigned)ntiles, detail::kGB, 0, q.cuda_stream()>>>(n, first, pred, cnt);
-  detail::counts_scan_kernel<<<1, 1, 0, q.cuda_stream()>>>(ntiles, cnt, num_elements_copied);
+  detail::counts_scan_kernel<<<1, detail::kGB, 0, q.cuda_stream()>>>(ntiles, cnt, num_elements_copied);
   detail::tile_compact_kernel<<<(unsigned)ntiles, detail::kGB, 0, q.cuda_stream()>>>(n, first, pred, cnt, d_first);
   b2p_sycl::detail::check_cuda(cudaGetLastError(), "copy_if");
   return q.record();

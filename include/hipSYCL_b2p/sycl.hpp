@@ -50,6 +50,9 @@
 #include <vector>
 
 #include "../b2p.h"
+#include "../b2p_device/reduce.cuh"
+
+#include <mutex>
 
 #define B2P_HD __host__ __device__
 
@@ -912,6 +915,107 @@ __global__ void __launch_bounds__(1) reduction_final_kernel(int nb, Op op, const
   }
 }
 
+// ------------------------------ reductions on the library's reduce kernel
+//
+// parallel_for(range, reduction(var, op), kernel) for a standard operator
+// (plus, multiplies, minimum, maximum, bit_and/or/xor) on int32/uint32/
+// int64/uint64/float/double runs the single-pass reduce kernel of libb2p
+// (b2p_device/reduce.cuh) with the user kernel as its source: unit i calls
+// kernel(id<1>(i), reducer) on a fresh reducer and folds the reducer's value
+// into the lane's accumulator -- compensated (TwoSum) for float plus, and in
+// a fixed combination order, so the result is the same for every launch.
+// Other types and user operators take the generic kernels above.
+
+template <class T>
+constexpr int b2p_dtype() {
+  if constexpr (std::is_same_v<T, float>) return B2P_F32;
+  else if constexpr (std::is_same_v<T, double>) return B2P_F64;
+  else if constexpr (std::is_integral_v<T> && !std::is_same_v<T, bool> && sizeof(T) == 4)
+    return std::is_signed_v<T> ? B2P_I32 : B2P_U32;
+  else if constexpr (std::is_integral_v<T> && !std::is_same_v<T, bool> && sizeof(T) == 8)
+    return std::is_signed_v<T> ? B2P_I64 : B2P_U64;
+  else return -1;
+}
+
+template <class Op, class T>
+constexpr int b2p_op() {
+  constexpr bool is_int = std::is_integral_v<T>;
+  if constexpr (is_op<Op, plus>::value || is_op<Op, std::plus>::value) return B2P_SUM;
+  else if constexpr (is_op<Op, multiplies>::value || is_op<Op, std::multiplies>::value) return B2P_PROD;
+  else if constexpr (is_op<Op, minimum>::value) return B2P_MIN;
+  else if constexpr (is_op<Op, maximum>::value) return B2P_MAX;
+  else if constexpr (is_int && (is_op<Op, bit_and>::value || is_op<Op, std::bit_and>::value)) return B2P_AND;
+  else if constexpr (is_int && (is_op<Op, bit_or>::value || is_op<Op, std::bit_or>::value)) return B2P_OR;
+  else if constexpr (is_int && (is_op<Op, bit_xor>::value || is_op<Op, std::bit_xor>::value)) return B2P_XOR;
+  else return -1;
+}
+
+template <class T, class Op>
+constexpr bool library_reduction() {
+  return b2p_dtype<T>() >= 0 && b2p_op<Op, T>() >= 0;
+}
+
+template <class T, class Op>
+using library_policy = typename ::b2p::PolicyOf<b2p_dtype<T>(), b2p_op<Op, T>()>::type;
+
+// Unit i of a reduction kernel: the value one work-item's reducer holds
+// after kernel(id<1>(i), reducer) (or kernel(item<1>, reducer)).
+template <class T, class Op, class K>
+struct reduction_source : ::b2p::ValueSource<reduction_source<T, Op, K>, T> {
+  K k;
+  size_t n;
+  Op op;
+  T identity;
+  reduction_source(K k_, size_t n_, Op op_, T id_) : k(k_), n(n_), op(op_), identity(id_) {}
+  __device__ __forceinline__ T value(long long i) const {
+    reducer<T, Op> r(op, identity, true);
+    if constexpr (std::is_invocable_v<K, item<1>, reducer<T, Op> &>) k(item<1>{(size_t)i, n}, r);
+    else k(id<1>((size_t)i), r);
+    return r.value();
+  }
+};
+
+// Scratch of one queue for the library's kernels: grown on demand (the
+// queue waits for its own work before a larger buffer replaces the old one),
+// zero-filled on allocation, freed with the queue.  Calls on one queue run
+// in stream order, so they can share it.
+class queue_scratch {
+ public:
+  explicit queue_scratch(int dev) : dev_(dev) {}
+  queue_scratch(const queue_scratch &) = delete;
+  queue_scratch &operator=(const queue_scratch &) = delete;
+  ~queue_scratch() {
+    if (p_) {
+      device_guard g(dev_);
+      cudaFree(p_);
+      cudaGetLastError();
+    }
+  }
+  void *get(size_t bytes, cudaStream_t s) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (bytes > bytes_) {
+      device_guard g(dev_);
+      if (p_) {
+        check_cuda(cudaStreamSynchronize(s), "queue scratch");
+        cudaFree(p_);
+        p_ = nullptr;
+      }
+      const size_t b = std::max<size_t>(bytes, 64 * 1024);
+      check_cuda(cudaMalloc(&p_, b), "queue scratch");
+      check_cuda(cudaMemsetAsync(p_, 0, b, s), "queue scratch");
+      bytes_ = b;
+    }
+    return p_;
+  }
+  size_t size() const { return bytes_; }
+
+ private:
+  int dev_;
+  std::mutex mu_;
+  void *p_ = nullptr;
+  size_t bytes_ = 0;
+};
+
 }  // namespace detail
 
 class handler;
@@ -926,6 +1030,7 @@ class queue {
     cudaStream_t s = nullptr;
     detail::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = std::shared_ptr<CUstream_st>(s, [](cudaStream_t p) { cudaStreamDestroy(p); });
+    scratch_ = std::make_shared<detail::queue_scratch>(dev_.cuda_ordinal());
   }
   device get_device() const { return dev_; }
   cudaStream_t cuda_stream() const { return stream_.get(); }
@@ -994,6 +1099,19 @@ class queue {
     depends_on(deps);
     detail::device_guard g(dev_.cuda_ordinal());
     const size_t n = r.size();
+    if constexpr (detail::library_reduction<T, Op>()) {
+      if (red.has_identity && n > 0) {
+        using P = detail::library_policy<T, Op>;
+        detail::reduction_source<T, Op, K> src(k, n, red.op, red.identity);
+        const size_t bytes = ::b2p::reduce_gen_scratch_bytes(n);
+        void *s = scratch_->get(bytes, cuda_stream());
+        // initialize_to_identity: *var = identity op r; otherwise op(*var, r)
+        detail::check_b2p(::b2p::launch_reduce_gen<P>(src, n, red.var, red.init_to_identity ? &red.identity : nullptr,
+                                                      s, scratch_->size(), cuda_stream()),
+                          "parallel_for(reduction)");
+        return record();
+      }
+    }
     const int grid = n ? grid_for(n) : 1;
     T *partial = nullptr;
     int *partial_has = nullptr;
@@ -1025,6 +1143,7 @@ class queue {
  private:
   device dev_;
   std::shared_ptr<CUstream_st> stream_;
+  std::shared_ptr<detail::queue_scratch> scratch_;
 };
 
 // handler: the command-group form q.submit([&](handler& h) { ... }).

@@ -88,6 +88,7 @@ def _declare(L):
         "b2p_segmented_per_call": ([i, i, i, vp, vp, vp, i64, vp, sz, i, vp], i),
         "b2p_device_error": ([vp, vp, i], i),
         "b2p_set_wait_timeout_ns": ([u64], u64),
+        "b2p_wait_timeout_ns": ([], u64),
         "b2p_debug_stall_tile": ([i64], None),
         "b2p_plan_segmented": ([ctypes.POINTER(vp), i, i, i, vp, vp, vp, i64, sz, i, vp], i),
         "b2p_plan_launch": ([vp, vp], i),

@@ -2,7 +2,7 @@
 // and pointer validation, configuration resolution, and dispatch to the
 // kernel launchers.  Also the per-device caches (SM count, occupancy,
 // shared-memory attributes) the launchers use.
-#include "common.cuh"
+#include "b2p_device/common.cuh"
 #include "internal.h"
 
 #include <atomic>
@@ -375,6 +375,8 @@ int b2p_device_error(void *scratch, b2p_stream stream, int clear) {
 }
 
 uint64_t b2p_set_wait_timeout_ns(uint64_t ns) { return g_timeout_ns.exchange(ns ? ns : 1); }
+
+uint64_t b2p_wait_timeout_ns(void) { return g_timeout_ns.load(); }
 
 void b2p_debug_stall_tile(int64_t tile) { g_stall_tile.store(tile); }
 

@@ -22,10 +22,10 @@
 //                            31 counting warps work on landed chunks, so
 //                            loads stay in flight while the atomics run
 //                            (grid mode 1)
-#include "common.cuh"
+#include "b2p_device/common.cuh"
 #include "internal.h"
-#include "tile.cuh"
-#include "tma.cuh"
+#include "b2p_device/tile.cuh"
+#include "b2p_device/tma.cuh"
 
 #include <algorithm>
 

@@ -90,6 +90,18 @@ int launch_segmented(int prim, int dtype, int op, int inclusive, const void *in,
                      const int64_t *offsets, int64_t nseg, size_t total, const void *init,
                      void *scratch, size_t scratch_bytes, int config, cudaStream_t s);
 bool segmented_config_valid(int dtype, int config);
+// The pipelined segmented kernel (flat segmented scan on the TMA pipeline):
+// whether it has the (dtype, op, block, items) shape, the scratch it needs
+// (prefix, one status word per tile, then one 64-int record per tile), the
+// host computation of the records, and the launch.  The records must
+// already be in scratch; returns B2P_ERR_UNSUPPORTED, having launched
+// nothing, when the call does not fit.
+bool segmented_tma_shape(int dtype, int op, int block, int items);
+size_t segmented_tma_scratch(size_t n, int block, int items);
+void segmented_tile_records(const int64_t *offs, int64_t nseg, size_t n, int block, int items, int *rec);
+int launch_segmented_tma(int prim, int dtype, int op, int inclusive, const void *in, void *out,
+                         const int64_t *offsets, int64_t nseg, size_t n, const void *init, void *scratch,
+                         int block, int items, cudaStream_t s);
 
 // Element sizes.
 inline size_t dtype_size(int dtype) {

@@ -14,7 +14,7 @@
 // Host code only ever sees a host-side stand-in for the array's name; the
 // real device address comes from cudaGetSymbolAddress, with the device
 // current, and is passed to the kernel as a plain pointer.
-#include "common.cuh"
+#include "b2p_device/common.cuh"
 #include "internal.h"
 
 #include <mutex>

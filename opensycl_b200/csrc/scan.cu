@@ -29,7 +29,7 @@
 // fp32/bf16 SUM accumulates with compensated (TwoSum) arithmetic; scans
 // longer than 2^24 carry cross-tile prefixes in FP64.  All waits are bounded
 // and report B2P_ERR_TIMEOUT through the scratch error word.
-#include "scan_tile.cuh"
+#include "b2p_device/scan_tile.cuh"
 #include "internal.h"
 
 #include <algorithm>

@@ -26,9 +26,7 @@
 // last complete 128-byte row use plain loads and stores.  Every wait is
 // bounded; a wait that runs out records B2P_ERR_TIMEOUT in the scratch
 // header and the block leaves its loops.
-#include "scan_tile.cuh"
-#include "tma.cuh"
-#include "tmem.cuh"
+#include "b2p_device/copy_if.cuh"
 #include "internal.h"
 
 #include <algorithm>
@@ -37,424 +35,6 @@
 namespace b2p {
 
 namespace {
-
-constexpr int kMaxStages = 16;
-constexpr int kLookWarps = 2;
-// Bulk stores a store warp keeps in flight before it waits for the oldest
-// one to finish reading its stage (2 and 3 measured slower: a stage held by
-// a store is a stage the producer cannot fill).
-constexpr int kStoresInFlight = 1;
-// Fewest stages a pipelined launch runs with.
-constexpr int cmax(int a, int b) { return a > b ? a : b; }
-constexpr int kMinStages = cmax(3, cmax(kLookWarps, kStoresInFlight));
-constexpr size_t kSmemBudget = 210 * 1024;  // stages + thread prefixes
-// Scans stage tiles that wait for their carries in TMEM where the policy
-// and shape allow it.
-constexpr bool kUseTmem = true;
-// Output stages of the TMEM-staged copy_if.
-constexpr int kCopyOutStages = 2;
-// Output stages of the TMEM-staged scan, and the bulk tensor stores its
-// store warp keeps in flight (at most kScanOutStages - 1).
-constexpr int kScanOutStages = 2;
-constexpr int kTmemStoresInFlight = 1;
-constexpr int kScanMaxInStages = kMaxStages;
-
-// Threads of a pipelined block with NC reducer and NC emitter threads.
-constexpr int pipe_threads(int nc) { return 2 * nc + 32 * kLookWarps + 64; }
-
-struct TmaParams {
-  unsigned long long n;
-  long long ntiles;
-  long long rows_full;            // complete 128-byte input rows (the input tensor map's extent)
-  unsigned long long tail_begin;  // first element past the complete input rows
-  long long rows_full_out;        // complete 128-byte output rows (scans)
-  unsigned long long tail_out_begin;  // first element past the complete output rows
-  unsigned out_offset;            // byte offset of a stage's output tile (0: in place)
-  int inclusive;
-  int has_init;
-  unsigned long long init_raw;    // Out-typed init value
-  int stages;
-  unsigned stage_stride;          // bytes between stages
-  // TMEM-staged scan: carry slots in TMEM, output stages after the input
-  // stages, thread prefixes per slot after the output stages
-  int slots;
-  int out_stages;
-  unsigned out_stage_stride;
-  unsigned out_base;
-  unsigned texcl_base;
-  const void *in;
-  void *out;
-  ScratchHeader *hdr;
-  StatusWord *status;
-  unsigned long long timeout_ns;
-  long long stall_tile;
-  // copy_if
-  unsigned long long mask, rhs;
-  int cmp;
-  unsigned long long *num_copied;
-};
-
-// Block-shared state of the pipeline.  Per stage: the TMA fill barrier
-// (full: producer -> reducers), aggregate published (aggr: reducers ->
-// look-back warps), carry known (cready: look-back warps -> emitters),
-// outputs in place (emitted: emitters -> store warp), stage free (empty:
-// store warp -> producer); the stage's tile id, aggregate and carry.
-struct PipeState {
-  uint64_t full[kMaxStages], empty[kMaxStages], aggr[kMaxStages], cready[kMaxStages], emitted[kMaxStages];
-  long long tile[kMaxStages];
-  // TMEM-staged scan: slot handed back by the emitters, output stage handed
-  // back by the store warp, tile ids of input and output stages, TMEM base
-  uint64_t slot_free[kMaxStages], out_empty[kMaxStages], slot_ready[kMaxStages];
-  long long tile_in[kMaxStages], tile_out[kMaxStages];
-  unsigned long long out_carry[kMaxStages], out_count[kMaxStages];  // copy_if: output stage's position, count
-  uint32_t tmem_base;
-  unsigned long long agg[kMaxStages], carry[kMaxStages];
-  unsigned long long epoch;
-  long long end_item;  // number of tiles this block handles, once the reducers know it
-};
-
-
-// --------------------------------------------------- per-thread tile passes
-// `t` is the thread's index inside its warp group (reducers or emitters).
-
-template <class P, int ITEMS>
-__device__ __forceinline__ typename P::Acc thread_total_t(const char *buf, int t) {
-  using In = typename P::In;
-  constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int VPT = ITEMS * (int)sizeof(In) / 16;
-  typename P::Acc agg = P::identity();
-#pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&w);
-#pragma unroll
-    for (int q = 0; q < IPV; ++q) P::add(agg, e[q]);
-  }
-  if constexpr (P::kCompensated) agg = df_norm(agg);
-  return agg;
-}
-
-// fp32 / bf16-input SUM, reducer pass: compensated (TwoSum) running sums of
-// the thread's elements from zero, rounded to fp32 and written to the
-// stage's output tile (in place for fp32 input; inclusive: after adding the
-// element, exclusive: before).  Returns the thread total.
-template <class In, int ITEMS, bool INCLUSIVE>
-__device__ __forceinline__ DF thread_runs(const char *inbuf, char *outbuf, int t) {
-  constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int VPT_IN = ITEMS / IPV, VPT_OUT = ITEMS / 4, OPI = IPV / 4;
-  DF run{0.f, 0.f};
-#pragma unroll
-  for (int k = 0; k < VPT_IN; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT_IN + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&w);
-#pragma unroll
-    for (int m = 0; m < OPI; ++m) {
-      float4 o;
-      float *oe = reinterpret_cast<float *>(&o);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float x;
-        if constexpr (sizeof(In) == 2) x = bf16_bits_to_f32(e[m * 4 + q]);
-        else x = e[m * 4 + q];
-        if constexpr (INCLUSIVE) {
-          df_accumulate(run, x);
-          oe[q] = __fadd_rn(run.hi, run.lo);
-        } else {
-          oe[q] = __fadd_rn(run.hi, run.lo);
-          df_accumulate(run, x);
-        }
-      }
-      *reinterpret_cast<float4 *>(outbuf + swz(t * VPT_OUT + k * OPI + m) * 16) = o;
-    }
-  }
-  (void)VPT_OUT;
-  return df_norm(run);
-}
-
-// fp32 SUM, emitter pass: output = start + run.  The run carries at most one
-// rounding of its exact value, so each output is within ~2 ulp of the exact
-// prefix for same-signed data.
-template <int ITEMS>
-__device__ __forceinline__ void emit_f32_runs(char *buf, DF start, int t) {
-  constexpr int VPT = ITEMS / 4;
-#pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    float4 *slot = reinterpret_cast<float4 *>(buf + swz(t * VPT + k) * 16);
-    float4 w = *slot;
-    w.x = __fadd_rn(start.hi, __fadd_rn(start.lo, w.x));
-    w.y = __fadd_rn(start.hi, __fadd_rn(start.lo, w.y));
-    w.z = __fadd_rn(start.hi, __fadd_rn(start.lo, w.z));
-    w.w = __fadd_rn(start.hi, __fadd_rn(start.lo, w.w));
-    *slot = w;
-  }
-}
-
-// Generic emitter pass: the thread's outputs from its running value, into
-// the stage's output tile (in place when input and output sizes match; each
-// output vector overwrites only input this thread has already read).
-template <class P, int ITEMS>
-__device__ __forceinline__ void emit_generic(const char *inbuf, char *outbuf, typename P::Acc run, bool inclusive,
-                                             int t) {
-  using In = typename P::In;
-  using Out = typename P::Out;
-  constexpr int IPV = 16 / (int)sizeof(In);
-  constexpr int OPV = 16 / (int)sizeof(Out);
-  constexpr int VPT_IN = ITEMS / IPV, VPT_OUT = ITEMS / OPV, OPI = IPV / OPV;
-#pragma unroll
-  for (int k = 0; k < VPT_IN; ++k) {
-    const uint4 w = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT_IN + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&w);
-#pragma unroll
-    for (int m = 0; m < OPI; ++m) {
-      uint4 o;
-      Out *oe = reinterpret_cast<Out *>(&o);
-#pragma unroll
-      for (int q = 0; q < OPV; ++q) {
-        if (inclusive) {
-          P::add(run, e[m * OPV + q]);
-          oe[q] = P::finalize(run);
-        } else {
-          oe[q] = P::finalize(run);
-          P::add(run, e[m * OPV + q]);
-        }
-      }
-      *reinterpret_cast<uint4 *>(outbuf + swz(t * VPT_OUT + k * OPI + m) * 16) = o;
-    }
-  }
-}
-
-// Exclusive scan over one warp group of NC threads (named barrier `bar`);
-// t = index in the group.
-template <class Ops, int NC>
-__device__ __forceinline__ typename Ops::Pub group_exclusive_scan(typename Ops::Pub v, typename Ops::Pub *s_warp,
-                                                                  typename Ops::Pub *total, int t, int bar) {
-  using Pub = typename Ops::Pub;
-  constexpr int kWarps = NC / 32;
-  const int lane = t & 31, warp = t >> 5;
-  Pub incl = v;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    Pub o = shfl_up(incl, d);
-    if (lane >= d) incl = Ops::combine(o, incl);
-  }
-  if (lane == 31) s_warp[warp] = incl;
-  bar_named(bar, NC);
-  if (warp == 0) {
-    Pub w = lane < kWarps ? s_warp[lane] : Ops::identity();
-#pragma unroll
-    for (int d = 1; d < kWarps; d <<= 1) {
-      Pub o = shfl_up(w, d);
-      if (lane >= d) w = Ops::combine(o, w);
-    }
-    if (lane < kWarps) s_warp[lane] = w;
-  }
-  bar_named(bar, NC);
-  Pub ex = shfl_up(incl, 1);
-  if (lane == 0) ex = Ops::identity();
-  if (warp > 0) ex = Ops::combine(s_warp[warp - 1], ex);
-  *total = s_warp[kWarps - 1];
-  return ex;  // callers end with a bar_named(bar, NC) before s_warp is used again
-}
-
-// Exclusive scan over one warp group of NC threads with a single named
-// barrier: after the warp totals are in s_warp, every warp scans them itself
-// (the same combine tree warp 0 runs in group_exclusive_scan, so the same
-// bits).  s_warp may be written again only after a later barrier of the
-// group.
-template <class Ops, int NC>
-__device__ __forceinline__ typename Ops::Pub group_exclusive_scan_1bar(typename Ops::Pub v,
-                                                                       typename Ops::Pub *s_warp,
-                                                                       typename Ops::Pub *total, int t, int bar) {
-  using Pub = typename Ops::Pub;
-  constexpr int kWarps = NC / 32;
-  const int lane = t & 31, warp = t >> 5;
-  Pub incl = v;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    Pub o = shfl_up(incl, d);
-    if (lane >= d) incl = Ops::combine(o, incl);
-  }
-  if (lane == 31) s_warp[warp] = incl;
-  bar_named(bar, NC);
-  Pub w = lane < kWarps ? s_warp[lane] : Ops::identity();
-#pragma unroll
-  for (int d = 1; d < kWarps; d <<= 1) {
-    Pub o = shfl_up(w, d);
-    if (lane >= d) w = Ops::combine(o, w);
-  }
-  const Pub before = shfl_idx(w, warp > 0 ? warp - 1 : 0);
-  *total = shfl_idx(w, kWarps - 1);
-  Pub ex = shfl_up(incl, 1);
-  if (lane == 0) ex = Ops::identity();
-  if (warp > 0) ex = Ops::combine(before, ex);
-  return ex;
-}
-
-// Carry of tile 0 (init, or the identity), in the published representation.
-template <class P, bool WIDE>
-__device__ __forceinline__ unsigned long long tile0_carry(const TmaParams &p) {
-  using Out = typename P::Out;
-  if (!p.has_init) {
-    if constexpr (WIDE) return F64Ops::pack(0.0);
-    else return P::pack(P::identity());
-  }
-  const Out v = from_bits64<Out>(p.init_raw);
-  if constexpr (WIDE) return F64Ops::pack((double)v);
-  else return P::pack(P::from_out(v));
-}
-
-// ------------------------------------------------------------ warp roles
-
-// Thread 0 of the block: barriers and the launch epoch.
-__device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < p.stages; ++i) {
-      mbar_init(&ps.full[i], 1);
-      mbar_init(&ps.empty[i], 1);
-      mbar_init(&ps.aggr[i], 1);
-      mbar_init(&ps.cready[i], 1);
-      mbar_init(&ps.emitted[i], 1);
-    }
-    mbar_init_fence();
-    ps.epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
-    ps.end_item = 0x7fffffffffffffffll;
-  }
-}
-
-// Producer (one thread): each tile's complete rows into the next free stage
-// in boxes of `box` rows.  A tile wholly past the complete rows completes
-// its stage without a copy.  Tile id -1 ends the reducers.
-__device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaParams &p, PipeState &ps,
-                                              char *smem, int rows, int box, long long *tiles) {
-  prefetch_tensormap(tin);
-  const unsigned long long pol = l2_policy_stream();
-  const int S = p.stages;
-  for (RingPos r;; r.advance(1, S)) {
-    const int s = r.s;
-    if (!mbar_wait(&ps.empty[s], r.ph ^ 1u, p.timeout_ns)) {
-      record_error(p.hdr, B2P_ERR_TIMEOUT);
-      tiles[s] = -1;
-      mbar_arrive(&ps.full[s]);
-      return;
-    }
-    const long long tile = (long long)atomicAdd(&p.hdr->tile_ctr, 1ull);
-    if (tile >= p.ntiles) {
-      tiles[s] = -1;
-      mbar_arrive(&ps.full[s]);
-      return;
-    }
-    tiles[s] = tile;
-    const long long r0 = tile * rows;
-    const long long rows_in = min((long long)rows, p.rows_full - r0);
-    const int nbox = rows_in > 0 ? (int)((rows_in + box - 1) / box) : 0;
-    if (nbox == 0) {
-      mbar_arrive(&ps.full[s]);
-    } else {
-      mbar_arrive_expect_tx(&ps.full[s], (unsigned)nbox * (unsigned)box * 128u);
-      for (int b = 0; b < nbox; ++b)
-        tma_load_2d(smem + (size_t)s * p.stage_stride + (size_t)b * box * 128, tin, 0,
-                    (int)(r0 + (long long)b * box), &ps.full[s], pol);
-    }
-  }
-}
-
-// Look-back warp wi of kLookWarps: items wi, wi + kLookWarps, ... in stage
-// order.  Resolves each reduced tile's carry, publishes its inclusive prefix
-// and hands the carry to the emitters.
-template <class Ops>
-__device__ __forceinline__ void lookback_loop(const TmaParams &p, PipeState &ps, int wi,
-                                              unsigned long long init_bits, unsigned long long epoch_tag, int S) {
-  using Pub = typename Ops::Pub;
-  const int lane = threadIdx.x & 31;
-  RingPos r;
-  r.advance(wi, S);
-  for (long long it = wi;; it += kLookWarps, r.advance(kLookWarps, S)) {
-    const int s = r.s;
-    const bool ok = __shfl_sync(0xffffffffu, (int)mbar_wait(&ps.aggr[s], r.ph, p.timeout_ns), 0) != 0;
-    if (!ok) {
-      if (lane == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-      return;
-    }
-    if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) return;
-    const long long tile = ps.tile[s];
-    const unsigned long long agg_bits = ps.agg[s];
-    Pub carry = Ops::unpack(init_bits);
-    if (tile > 0) {
-      bool err;
-      // tile 0's prefix includes init, so the look-back result already does
-      carry = lookback<Ops, false>(p.status, tile, epoch_tag, p.timeout_ns, err);
-      if (lane == 0) {
-        if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        if (tile != p.stall_tile)
-          st_status(p.status + tile, Ops::pack(Ops::combine(carry, Ops::unpack(agg_bits))),
-                    epoch_tag | kFlagPrefix | (err ? kFlagError : 0));
-      }
-    }
-    if (lane == 0) {
-      ps.carry[s] = Ops::pack(carry);
-      mbar_arrive(&ps.cready[s]);
-    }
-    __syncwarp();
-  }
-}
-
-// Emitter group: wait for item `it`'s carry, or learn that the block's items
-// are exhausted (the reducers publish the count when they meet the end).
-// Returns 1 = carry ready, 0 = no more items, -1 = timeout.
-__device__ __forceinline__ int emitter_wait(const TmaParams &p, PipeState &ps, const RingPos &r, long long it) {
-  uint64_t t0 = 0;
-  for (unsigned k = 0;; ++k) {
-    if (mbar_try(&ps.cready[r.s], r.ph)) return 1;
-    if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) return 0;
-    if ((k & 31) == 31) {
-      const uint64_t now = globaltimer_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > p.timeout_ns) return -1;
-    }
-  }
-}
-
-// Emitter leader after the last item (`it` = item count): every earlier item
-// passed the look-back warps and was handed to the store warp, so their
-// barriers are in step; end the look-back warps (waiting on items it and
-// it + 1) and the store warp (waiting on item it).
-__device__ __forceinline__ void emitters_finish(const TmaParams &p, PipeState &ps, RingPos r) {
-  mbar_arrive(&ps.emitted[r.s]);
-  for (int j = 0; j < kLookWarps; ++j, r.advance(1, p.stages)) mbar_arrive(&ps.aggr[r.s]);
-}
-
-// Store warp: stages whose bulk stores were committed but may still read
-// shared memory.  A stage is handed back to the producer (empty barrier)
-// once its store has read it; up to kStoresInFlight stores overlap.
-template <int D = kStoresInFlight>
-struct StoreRelease {
-  RingPos oldest;
-  int pending = 0;
-  // after committing a store group for the ring of S barriers `freed`
-  __device__ __forceinline__ void committed(uint64_t *freed, int S) {
-    if (++pending < D) return;
-    bulk_wait_read<D - 1>();
-    mbar_arrive(&freed[oldest.s]);
-    oldest.advance(1, S);
-    --pending;
-  }
-  __device__ __forceinline__ void drain(uint64_t *freed, int S) {
-    bulk_wait_read<0>();
-    for (; pending > 0; --pending, oldest.advance(1, S)) mbar_arrive(&freed[oldest.s]);
-  }
-};
-
-// Elements past the complete rows (only in the last tile) into the stage,
-// by the reducer group (threads 0 .. ntail-1 of the block).
-template <class T, int NC>
-__device__ __forceinline__ void load_row_tail(const TmaParams &p, char *buf, long long tile, int tile_elems) {
-  const int ntail = (int)(p.n - p.tail_begin);
-  const long long j0 = (long long)p.tail_begin - tile * tile_elems;
-  if ((int)threadIdx.x < ntail)
-    *smem_elem_ptr<T>(buf, (int)j0 + (int)threadIdx.x) =
-        reinterpret_cast<const T *>(p.in)[p.tail_begin + threadIdx.x];
-  bar_named(1, NC);
-}
 
 // ------------------------------------------------------------------- scan
 
@@ -606,20 +186,6 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
 // tiles on their way in and out, while up to 512 / kSlotCols tiles wait for
 // their carries in TMEM.
 
-// Policies whose outputs the TMEM kernel forms as combine(start, run) with
-// the bits of the in-place kernel's sequential pass: integer operators (exact
-// in wrap-around arithmetic) and fp32 / bf16-input SUM (the same
-// start.hi + (start.lo + run) formula).  Floating-point PROD, MIN, MAX and
-// fp64 SUM stay on the in-place kernel.
-template <class P>
-struct TmemExact : std::integral_constant<bool, P::kCompensated || std::is_integral<typename P::Acc>::value> {};
-
-// TMEM columns a reducer thread fills per tile.
-template <class P, int ITEMS>
-constexpr int tmem_cols() {
-  return ITEMS * (int)sizeof(typename P::Out) / 4;
-}
-
 // Reducer pass: the thread's ITEMS elements from the landed stage, their
 // running values from the identity (inclusive: after adding the element,
 // exclusive: before) as 32-bit words for TMEM, and the thread total.
@@ -679,31 +245,6 @@ __device__ __forceinline__ void tmem_emit(const uint32_t *w, typename P::Acc sta
       else oe[q] = P::finalize(P::combine(start, P::from_out(r)));
     }
     *reinterpret_cast<uint4 *>(obuf + swz(t * VPT + k) * 16) = u;
-  }
-}
-
-// Thread 0: barriers of the three rings (input stages, TMEM slots, output
-// stages) and the launch epoch.  Reducer and emitter warps arrive one by one
-// on the barriers that hand back input stages and slots.
-__device__ __forceinline__ void tmem_pipe_init(PipeState &ps, const TmaParams &p, unsigned group_warps) {
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < p.stages; ++i) {
-      mbar_init(&ps.full[i], 1);
-      mbar_init(&ps.empty[i], group_warps);
-    }
-    for (int i = 0; i < p.slots; ++i) {
-      mbar_init(&ps.aggr[i], 1);
-      mbar_init(&ps.cready[i], 1);
-      mbar_init(&ps.slot_free[i], group_warps);
-      mbar_init(&ps.slot_ready[i], group_warps);
-    }
-    for (int i = 0; i < p.out_stages; ++i) {
-      mbar_init(&ps.emitted[i], 1);
-      mbar_init(&ps.out_empty[i], 1);
-    }
-    mbar_init_fence();
-    ps.epoch = *reinterpret_cast<volatile unsigned long long *>(&p.hdr->epoch);
-    ps.end_item = 0x7fffffffffffffffll;
   }
 }
 
@@ -1081,277 +622,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   finish_launch(p.hdr, epoch, nullptr, 0);
 }
 
-// -------------------------------------------------- copy_if, TMEM-staged
-//
-// copy_if_tma_kernel's compaction with the TMEM staging of scan_tmem_kernel:
-// reducers park each thread's raw elements in a TMEM slot (keep masks and
-// thread offsets beside it in shared memory) and hand the input stage back
-// at once; emitters pack the kept elements into an output stage.
-//
-// Thread t owns elements t * ITEMS .. t * ITEMS + ITEMS - 1 (16-byte reads
-// of the swizzled stage) and packs them in order.  Both groups work through
-// one tile at a time, so the per-element work is kept to a few instructions;
-// the price is bank conflicts in the packing stores for regular keep patterns
-// (every lane keeping 32 elements puts all 32 lanes of a store on one bank),
-// where the pipeline falls to about 1.8 TB/s.  A warp-striped layout with
-// ballot packing, and lane-rotated element order, were both measured: free
-// of conflicts, but slower at typical selectivities.
-
-// Keep bits of a thread's ITEMS elements (w: the elements as 32-bit words,
-// element j at tile index first + j); only the first `count` elements of the
-// tile are real.
-template <class T, int ITEMS, int CMP>
-__device__ __forceinline__ unsigned keep_bits(const uint32_t *w, unsigned long long mask64,
-                                              unsigned long long rhs64, int first, int count) {
-  using U = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned>::type;
-  const U mask = (U)mask64, rhs = (U)rhs64;
-  unsigned keep = 0;
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    U e;
-    memcpy(&e, w + j * (int)(sizeof(T) / 4), sizeof(T));
-    const U a = e & mask;
-    bool kb;
-    if constexpr (CMP == B2P_CMP_LT) kb = a < rhs;
-    else if constexpr (CMP == B2P_CMP_LE) kb = a <= rhs;
-    else if constexpr (CMP == B2P_CMP_EQ) kb = a == rhs;
-    else if constexpr (CMP == B2P_CMP_NE) kb = a != rhs;
-    else if constexpr (CMP == B2P_CMP_GE) kb = a >= rhs;
-    else kb = a > rhs;
-    keep |= (unsigned)kb << j;
-  }
-  if (count < first + ITEMS) keep &= count <= first ? 0u : ((1u << (count - first)) - 1u);  // count - first < 32 here
-  return keep;
-}
-
-template <class T, int NC, int ITEMS, int CMP>
-__global__ void __launch_bounds__(pipe_threads(NC), 1)
-    copy_if_tmem_kernel(const __grid_constant__ CUtensorMap tin, TmaParams p) {
-  constexpr int kTile = NC * ITEMS;
-  constexpr int kEpr = 128 / (int)sizeof(T);
-  static_assert(kTile % (8 * kEpr) == 0, "a stage is a whole number of 1024-byte swizzle atoms");
-  constexpr int kRows = kTile / kEpr;
-  constexpr int kBox = kRows < 256 ? kRows : 256;
-  static_assert(kRows % kBox == 0, "box rows");
-  static_assert(ITEMS <= 32, "keep mask is 32 bits");
-  static_assert(kTile <= 65536, "thread offsets are 16 bits");
-  constexpr int kCols = ITEMS * (int)sizeof(T) / 4;
-  static_assert(kCols == 16 || kCols == 32, "TMEM columns per thread");
-  static_assert(NC % 128 == 0, "reducer and emitter groups cover the four TMEM lane quarters evenly");
-  constexpr int kSlotCols = kCols * (NC / 128);
-
-  extern __shared__ char smem_raw[];
-  char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  char *obase = smem + p.out_base;
-  unsigned *keep_all = reinterpret_cast<unsigned *>(smem + p.texcl_base);
-  uint16_t *texcl_all = reinterpret_cast<uint16_t *>(keep_all + (size_t)p.slots * NC);  // offsets < 2^16
-  __shared__ __align__(8) PipeState ps;
-  __shared__ unsigned long long s_warp[32];
-  __shared__ int s_go[2];
-
-  const int warp = threadIdx.x >> 5;
-  tmem_pipe_init(ps, p, NC / 32);
-  if (warp == 0) {
-    __syncwarp();
-    tmem_alloc(&ps.tmem_base, 512);
-  }
-  tmem_fence_before();
-  __syncthreads();
-  tmem_fence_after();
-  const uint32_t tbase = ps.tmem_base;
-  const unsigned long long epoch = ps.epoch;
-  const unsigned long long epoch_tag = epoch << 8;
-  const int SI = p.stages, SL = p.slots, SO = p.out_stages;
-  const long long last = p.ntiles - 1;
-  const int ntail = (int)(p.n - p.tail_begin);
-  T *out = reinterpret_cast<T *>(p.out);
-
-  if (warp < NC / 32) {
-    // ------------------------------------------------------------ reducers
-    const int t = threadIdx.x;
-    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * kCols);
-    long long it = 0;
-    RingPos ri, rs;
-    for (;; ++it, ri.advance(1, SI), rs.advance(1, SL)) {
-      if (t == 0) {
-        int go = mbar_wait(&ps.full[ri.s], ri.ph, p.timeout_ns) ? 1 : -1;
-        if (go > 0 && ps.tile_in[ri.s] < 0) go = 0;
-        if (go > 0 && !mbar_wait(&ps.slot_free[rs.s], rs.ph ^ 1u, p.timeout_ns)) go = -1;
-        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        s_go[0] = go;
-      }
-      bar_named(1, NC);
-      if (s_go[0] <= 0) break;
-      (void)mbar_try(&ps.full[ri.s], ri.ph);  // completed: this thread's acquire of the TMA bytes
-      tmem_fence_after();
-      const long long tile = ps.tile_in[ri.s];
-      char *buf = smem + (size_t)ri.s * p.stage_stride;
-      if (tile == last && ntail > 0) load_row_tail<T, NC>(p, buf, tile, kTile);
-      uint32_t w[kCols];
-#pragma unroll
-      for (int k = 0; k < kCols / 4; ++k) {
-        const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * (kCols / 4) + k) * 16);
-        w[4 * k] = u.x;
-        w[4 * k + 1] = u.y;
-        w[4 * k + 2] = u.z;
-        w[4 * k + 3] = u.w;
-      }
-      __syncwarp();
-      if ((t & 31) == 0) mbar_arrive(&ps.empty[ri.s]);  // this warp is done with the input stage
-      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
-      tmem_st16(ta, w);
-      if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
-      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
-      const unsigned keep = keep_bits<T, ITEMS, CMP>(w, p.mask, p.rhs, t * ITEMS, count);
-      unsigned long long tile_kept;
-      const unsigned long long ex =
-          group_exclusive_scan<CountOps, NC>((unsigned long long)__popc(keep), s_warp, &tile_kept, t, 1);
-      texcl_all[(size_t)rs.s * NC + t] = (uint16_t)ex;
-      keep_all[(size_t)rs.s * NC + t] = keep;
-      tmem_wait_st();
-      tmem_fence_before();
-      bar_named(1, NC);  // slot, keep masks and offsets complete
-      if (t == 0) {
-        if (tile != p.stall_tile)
-          st_status(p.status + tile, tile_kept, epoch_tag | (tile == 0 ? kFlagPrefix : kFlagAgg));
-        ps.tile[rs.s] = tile;
-        ps.agg[rs.s] = tile_kept;
-        mbar_arrive(&ps.aggr[rs.s]);
-      }
-    }
-    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
-  } else if (warp < 2 * NC / 32) {
-    // ------------------------------------------------------------ emitters
-    const int t = threadIdx.x - NC;
-    const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(((t >> 5) >> 2) * kCols);
-    RingPos rs, ro;
-    for (long long it = 0;; ++it, rs.advance(1, SL), ro.advance(1, SO)) {
-      if (t == 0) {
-        int go = emitter_wait(p, ps, rs, it);
-        if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
-        if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        if (go == 0) {
-          mbar_arrive(&ps.emitted[ro.s]);
-          RingPos r = rs;
-          for (int j = 0; j < kLookWarps; ++j, r.advance(1, SL)) mbar_arrive(&ps.aggr[r.s]);
-        }
-        s_go[1] = go;
-      }
-      bar_named(2, NC);
-      if (s_go[1] <= 0) break;
-      tmem_fence_after();
-      const long long tile = ps.tile[rs.s];
-      const unsigned long long carry = ps.carry[rs.s];
-      unsigned long long kept_total = ps.agg[rs.s];
-      if (carry > p.n || kept_total > p.n - carry) {  // only after a broken chain: write nothing
-        if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        kept_total = 0;
-      }
-      const unsigned keep = keep_all[(size_t)rs.s * NC + t];
-      const unsigned o = texcl_all[(size_t)rs.s * NC + t];
-      uint32_t w[kCols];
-      const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
-      if constexpr (kCols == 32) tmem_load32(ta, w);
-      else tmem_load16(ta, w);
-      tmem_fence_before();
-      __syncwarp();
-      if ((t & 31) == 0) mbar_arrive(&ps.slot_free[rs.s]);  // slot, masks and offsets read
-      char *obuf = obase + (size_t)ro.s * p.out_stage_stride;
-      const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
-      const unsigned phase = (unsigned)(g0 & 15u);
-      const unsigned lim = (unsigned)kept_total;
-#pragma unroll
-      for (int j = 0; j < ITEMS; ++j) {
-        const unsigned pos = o + __popc(keep & ((1u << j) - 1u));
-        if (((keep >> j) & 1u) && pos < lim) {
-          T v;
-          memcpy(&v, w + j * (int)(sizeof(T) / 4), sizeof(T));
-          *reinterpret_cast<T *>(obuf + phase + pos * sizeof(T)) = v;  // phase is a multiple of sizeof(T)
-        }
-      }
-      fence_async_smem();
-      bar_named(2, NC);
-      const uintptr_t g1 = g0 + kept_total * sizeof(T);
-      const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
-      const bool mid = a1 > a0;
-      const long long nhead = mid ? (long long)((a0 - g0) / sizeof(T)) : (long long)kept_total;
-      const long long tail0 = mid ? (long long)((a1 - g0) / sizeof(T)) : (long long)kept_total;
-      const long long ntl = (long long)kept_total - tail0;
-      if (t < nhead) out[carry + t] = *reinterpret_cast<const T *>(obuf + phase + t * sizeof(T));
-      if (t >= 32 && t - 32 < ntl) {
-        const long long k = tail0 + (t - 32);
-        out[carry + k] = *reinterpret_cast<const T *>(obuf + phase + k * sizeof(T));
-      }
-      if (t == 0 && tile == last && p.num_copied) *p.num_copied = carry + kept_total;
-      bar_named(2, NC);  // the plain stores are done with the output stage
-      if (t == 0) {
-        ps.out_carry[ro.s] = carry;
-        ps.out_count[ro.s] = kept_total;
-        mbar_arrive(&ps.emitted[ro.s]);
-      }
-    }
-  } else if (warp < 2 * NC / 32 + kLookWarps) {
-    lookback_loop<CountOps>(p, ps, warp - 2 * NC / 32, 0ull, epoch_tag, SL);
-  } else if (warp == 2 * NC / 32 + kLookWarps) {
-    if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile_in);
-  } else {
-    // ---------------------------------------------------------- store warp
-    if ((threadIdx.x & 31) == 0) {
-      RingPos ro;
-      for (long long it = 0;; ++it, ro.advance(1, SO)) {
-        if (!mbar_wait(&ps.emitted[ro.s], ro.ph, p.timeout_ns)) {
-          record_error(p.hdr, B2P_ERR_TIMEOUT);
-          break;
-        }
-        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
-        const unsigned long long carry = ps.out_carry[ro.s];
-        const unsigned long long kept_total = ps.out_count[ro.s];
-        const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
-        const uintptr_t g1 = g0 + kept_total * sizeof(T);
-        const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
-        if (a1 > a0) {
-          const char *src = obase + (size_t)ro.s * p.out_stage_stride + (g0 & 15u) + (a0 - g0);
-          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(a0),
-                       "r"(smem_u32(src)), "r"((unsigned)(a1 - a0))
-                       : "memory");
-        }
-        bulk_commit();
-        bulk_wait_read<0>();
-        mbar_arrive(&ps.out_empty[ro.s]);
-      }
-      bulk_wait_all();
-    }
-  }
-  tmem_fence_before();
-  __syncthreads();
-  if (warp == 0) {
-    tmem_fence_after();
-    tmem_dealloc(tbase, 512);
-  }
-  finish_launch(p.hdr, epoch, nullptr, 0);
-}
-
 // ------------------------------------------------------------------ host
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
-                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                  CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(f);
-    cudaGetLastError();
-  });
-  return fn;
-}
-
 template <class P, int NC, int ITEMS, bool WIDE>
 int launch_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &tout, cudaStream_t st) {
   auto kfn = scan_tma_kernel<P, NC, ITEMS, WIDE>;
@@ -1517,34 +788,17 @@ int launch_copy_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
-template <class T, int NC, int ITEMS, int CMP>
-int launch_copy_tmem_shape(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
-  constexpr int cols = ITEMS * (int)sizeof(T) / 4;
-  if constexpr (cols != 16 && cols != 32) {
-    return B2P_ERR_UNSUPPORTED;
-  } else {
-    auto kfn = copy_if_tmem_kernel<T, NC, ITEMS, CMP>;
-    const size_t smem = p.texcl_base + (size_t)p.slots * NC * 6 + 1024;
-    int rc = ensure_dynamic_smem((const void *)kfn, smem);
-    if (rc) return rc;
-    const int threads = pipe_threads(NC);
-    if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
-    const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
-    kfn<<<grid, threads, smem, st>>>(tin, p);
-    return cuda_status(cudaGetLastError());
-  }
-}
-
 template <class T, int NC, int ITEMS>
 int launch_copy_items(TmaParams &p, const CUtensorMap &tin, cudaStream_t st) {
   if (p.slots > 0) {
+    const int sms = device_info().sm_count;
     switch (p.cmp) {
-    case B2P_CMP_LT: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_LT>(p, tin, st);
-    case B2P_CMP_LE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_LE>(p, tin, st);
-    case B2P_CMP_EQ: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_EQ>(p, tin, st);
-    case B2P_CMP_NE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_NE>(p, tin, st);
-    case B2P_CMP_GE: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_GE>(p, tin, st);
-    default: return launch_copy_tmem_shape<T, NC, ITEMS, B2P_CMP_GT>(p, tin, st);
+    case B2P_CMP_LT: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_LT>{p.mask, p.rhs}, sms, st);
+    case B2P_CMP_LE: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_LE>{p.mask, p.rhs}, sms, st);
+    case B2P_CMP_EQ: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_EQ>{p.mask, p.rhs}, sms, st);
+    case B2P_CMP_NE: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_NE>{p.mask, p.rhs}, sms, st);
+    case B2P_CMP_GE: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_GE>{p.mask, p.rhs}, sms, st);
+    default: return launch_copy_tmem_shape<T, NC, ITEMS>(p, tin, MaskCmp<T, B2P_CMP_GT>{p.mask, p.rhs}, sms, st);
     }
   }
   switch (p.cmp) {
@@ -1563,31 +817,6 @@ int launch_copy_cmp(TmaParams &p, const CUtensorMap &tin, int block, int items, 
   if (block == 256 && items == 16) return launch_copy_items<T, 256, 16>(p, tin, st);
   if (block == 256 && items == 32) return launch_copy_items<T, 256, 32>(p, tin, st);
   return B2P_ERR_UNSUPPORTED;
-}
-
-// Shared-memory layout of the TMEM-staged copy_if for (block, items):
-// input stages, two output stages (a tile plus 1024 bytes for the output's
-// 16-byte phase), thread offsets and keep masks of every slot.  Leaves
-// p.slots = 0 (in-place kernel) when the shape has no TMEM kernel.
-bool copy_tmem_layout(TmaParams &p, size_t es, int block, int items) {
-  p.slots = 0;
-  if (!kUseTmem || (block != 128 && block != 256)) return false;
-  const int cols = items * (int)es / 4;
-  if (cols != 16 && cols != 32) return false;
-  const int slots = std::min(kMaxStages, 512 / (cols * block / 128));
-  const size_t in_b = (size_t)block * items * es, out_b = in_b + 1024;
-  const size_t side = ((size_t)slots * block * 6 + 1023) & ~size_t(1023);
-  const int so = kCopyOutStages;
-  if (so * out_b + side + 2 * in_b > kSmemBudget) return false;
-  const int si = (int)std::min<size_t>(kMaxStages, (kSmemBudget - so * out_b - side) / in_b);
-  p.stages = si;
-  p.stage_stride = (unsigned)in_b;
-  p.slots = slots;
-  p.out_stages = so;
-  p.out_stage_stride = (unsigned)out_b;
-  p.out_base = (unsigned)(si * in_b);
-  p.texcl_base = (unsigned)(si * in_b + so * out_b);
-  return true;
 }
 
 template <class T>
@@ -1625,19 +854,6 @@ int launch_copy_t(const void *in, void *out, size_t n, uint64_t mask, int cmp, u
 
 }  // namespace
 
-bool encode_row_tensor(CUtensorMap *map, const void *base, unsigned long long rows, int box_rows) {
-  EncodeTiledFn fn = encode_fn();
-  if (!fn || !base || (reinterpret_cast<uintptr_t>(base) & 15) || rows < 1 || rows >= (1ull << 31) ||
-      box_rows < 1 || box_rows > 256)
-    return false;
-  const cuuint64_t dims[2] = {128, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {128};
-  const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
 
 bool scan_tma_shape(int dtype, int block, int items) {
   if (dtype_size(dtype) == 0) return false;

@@ -15,7 +15,7 @@
 // Every piece is one work item fetched dynamically by persistent blocks.
 // Inside a piece, elements are scanned with the segmented operator
 // (flag, value): (f1, v1) + (f2, v2) = (f1 | f2, f2 ? v2 : v1 + v2).
-#include "tile.cuh"
+#include "b2p_device/scan_tile.cuh"
 #include "internal.h"
 #include "tuning.h"
 
@@ -54,29 +54,6 @@ struct SegParams {
   StatusWord *status;  // one word per piece
   unsigned long long timeout_ns;
 };
-
-// (flag, value) pair of the segmented operator.
-template <class P>
-struct SegPair {
-  typename P::Acc v;
-  int f;
-};
-
-template <class P>
-struct SegOps {
-  using Pub = SegPair<P>;
-  __device__ static Pub identity() { return Pub{P::identity(), 0}; }
-  __device__ static Pub combine(Pub a, Pub b) {
-    return Pub{b.f ? b.v : P::combine(a.v, b.v), a.f | b.f};
-  }
-};
-
-template <class P>
-__device__ __forceinline__ SegPair<P> shfl_up(SegPair<P> a, int d) {
-  a.v = shfl_up(a.v, d);
-  a.f = __shfl_up_sync(0xffffffffu, a.f, d);
-  return a;
-}
 
 template <class P, int ITEMS>
 __global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 8192 / ITEMS)
@@ -278,13 +255,15 @@ size_t pieces_upper_bound(size_t n, int64_t nseg, int cap) {
 
 size_t segmented_scratch_bytes(int dtype, size_t n, int64_t nseg, int config) {
   int cap = 512;  // smallest piece of the table
+  size_t flat = segmented_tma_scratch(n, 128, 16);  // smallest tile of the pipelined kernel
   if (config >= 0) {
     LaunchConfig lc = describe_config(config);
     cap = lc.block * lc.items;
+    flat = lc.grid_mode == 1 ? segmented_tma_scratch(n, lc.block, lc.items) : 0;
   }
   (void)dtype;
   const size_t np = pieces_upper_bound(n, nseg, cap);
-  return kScratchPrefix + np * (sizeof(StatusWord) + sizeof(Piece)) + 256;
+  return std::max(kScratchPrefix + np * (sizeof(StatusWord) + sizeof(Piece)), flat) + 256;
 }
 
 bool segmented_config_valid(int dtype, int config) { return seg_tile_ok(dtype, config); }
@@ -418,6 +397,34 @@ int seg_launch_with_pieces(int prim, int dtype, int op, int inclusive, const voi
 
 }  // namespace
 
+// Whether a call runs the pipelined flat kernel (seg_tma.cu): grid mode 1
+// with a shape it has, SUM, offsets starting at 0, 16-byte aligned input
+// (and output for a scan), at least one tile of elements.
+bool seg_tma_fits(int prim, int dtype, int op, int config, const void *in, const void *out, const int64_t *h,
+                  int64_t nseg, size_t total) {
+  const LaunchConfig lc = describe_config(config);
+  if (lc.grid_mode != 1 || !segmented_tma_shape(dtype, op, lc.block, lc.items)) return false;
+  if (h[0] != 0 || nseg >= (1ll << 31) - 2 || total < (size_t)lc.block * lc.items) return false;
+  if (reinterpret_cast<uintptr_t>(in) & 15) return false;
+  if (prim == B2P_PRIM_SEG_SCAN && (reinterpret_cast<uintptr_t>(out) & 15)) return false;
+  return true;
+}
+
+// The per-tile records of the pipelined kernel, copied into scratch after
+// its status words (synchronous: the records are a host temporary).
+int seg_tma_prepare(const int64_t *h, int64_t nseg, size_t total, int config, void *scratch, size_t scratch_bytes,
+                    cudaStream_t st) {
+  const LaunchConfig lc = describe_config(config);
+  if (scratch_bytes < segmented_tma_scratch(total, lc.block, lc.items)) return B2P_ERR_SCRATCH;
+  const size_t tile = (size_t)lc.block * lc.items, ntiles = (total + tile - 1) / tile;
+  std::vector<int> tk(ntiles * 64);
+  segmented_tile_records(h, nseg, total, lc.block, lc.items, tk.data());
+  char *dst = reinterpret_cast<char *>(scratch) + kScratchPrefix + ntiles * sizeof(StatusWord);
+  cudaError_t e = cudaMemcpyAsync(dst, tk.data(), tk.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return cuda_status(e);
+}
+
 int launch_segmented(int prim, int dtype, int op, int inclusive, const void *in, void *out,
                      const int64_t *offsets, int64_t nseg, size_t total, const void *init,
                      void *scratch, size_t scratch_bytes, int config, cudaStream_t st) {
@@ -433,6 +440,13 @@ int launch_segmented(int prim, int dtype, int op, int inclusive, const void *in,
   for (int64_t s = 0; s < nseg; ++s)
     if (h[(size_t)s + 1] < h[(size_t)s] || h[0] < 0) return B2P_ERR_INVALID_ARG;
   if ((size_t)h[(size_t)nseg] != total) return B2P_ERR_INVALID_ARG;
+  if (seg_tma_fits(prim, dtype, op, config, in, out, h.data(), nseg, total)) {
+    int rc = seg_tma_prepare(h.data(), nseg, total, config, scratch, scratch_bytes, st);
+    if (rc) return rc;
+    rc = launch_segmented_tma(prim, dtype, op, inclusive, in, out, offsets, nseg, total, init, scratch, lc.block,
+                              lc.items, st);
+    if (rc != B2P_ERR_UNSUPPORTED) return rc;
+  }
   std::vector<Piece> pieces = build_pieces(h.data(), nseg, cap);
   const size_t np = pieces.size();
   const size_t need = kScratchPrefix + np * (sizeof(StatusWord) + sizeof(Piece));
@@ -487,6 +501,7 @@ int b2p_plan_segmented(b2p_plan *plan, int prim, int dtype, int op, const void *
   }
   if (!seg_tile_ok(dtype, config)) return B2P_ERR_INVALID_ARG;
   LaunchConfig lc = describe_config(config);
+  const bool flat = seg_tma_fits(prim, dtype, op, config, in, out, h.data(), nseg, total_elems);
   std::vector<Piece> pieces = build_pieces(h.data(), nseg, lc.block * lc.items);
   const size_t np = pieces.size();
   b2p_plan_s *pl = new b2p_plan_s();
@@ -495,36 +510,65 @@ int b2p_plan_segmented(b2p_plan *plan, int prim, int dtype, int op, const void *
   pl->op = op;
   pl->config = config;
   pl->scratch_bytes = kScratchPrefix + np * (sizeof(StatusWord) + sizeof(Piece));
+  if (flat) pl->scratch_bytes = std::max(pl->scratch_bytes, segmented_tma_scratch(total_elems, lc.block, lc.items));
   e = cudaMalloc(&pl->scratch, pl->scratch_bytes);
-  if (e == cudaSuccess) e = cudaMemsetAsync(pl->scratch, 0, pl->scratch_bytes, st);
+  if (e != cudaSuccess) {
+    b2p_plan_destroy(pl);
+    return cuda_status(e);
+  }
   Piece *dp = reinterpret_cast<Piece *>(reinterpret_cast<char *>(pl->scratch) + kScratchPrefix +
                                         np * sizeof(StatusWord));
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, pieces.data(), np * sizeof(Piece), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    b2p_plan_destroy(pl);
-    return cuda_status(e);
+  // The flat kernel first; the piece kernel when the flat one turns out not
+  // to have the shape (its scratch contents differ, so each attempt fills the
+  // scratch before its capture).
+  int rc = B2P_ERR_UNSUPPORTED;
+  for (int attempt = flat ? 0 : 1; attempt < 2 && rc == B2P_ERR_UNSUPPORTED; ++attempt) {
+    const bool use_flat = attempt == 0;
+    e = cudaMemsetAsync(pl->scratch, 0, pl->scratch_bytes, st);
+    if (e == cudaSuccess && !use_flat)
+      e = cudaMemcpyAsync(dp, pieces.data(), np * sizeof(Piece), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      rc = cuda_status(e);
+      break;
+    }
+    if (use_flat) {
+      rc = seg_tma_prepare(h.data(), nseg, total_elems, config, pl->scratch, pl->scratch_bytes, st);
+      if (rc) break;
+    }
+    // capture the single launch into a graph
+    cudaStream_t cs;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      rc = cuda_status(e);
+      break;
+    }
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      if (use_flat)
+        rc = launch_segmented_tma(prim, dtype, op, 1, in, out, offsets, nseg, total_elems, nullptr, pl->scratch,
+                                  lc.block, lc.items, cs);
+      else
+        rc = seg_launch_with_pieces(prim, dtype, op, 1, in, out, offsets, nseg, nullptr, dp, (long long)np,
+                                    pl->scratch, config, cs);
+      cudaGraph_t g = nullptr;
+      cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+      if (rc == B2P_OK && e2 == cudaSuccess) {
+        pl->graph = g;
+        e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+      } else {
+        if (g) cudaGraphDestroy(g);
+        if (rc == B2P_OK) e = e2;
+      }
+    } else {
+      rc = B2P_OK;
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) rc = cuda_status(e);
   }
-  // capture the single launch into a graph
-  cudaStream_t cs;
-  e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-  if (e != cudaSuccess) {
+  if (rc != B2P_OK) {
     b2p_plan_destroy(pl);
-    return cuda_status(e);
-  }
-  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-  int rc = B2P_OK;
-  if (e == cudaSuccess) {
-    rc = seg_launch_with_pieces(prim, dtype, op, 1, in, out, offsets, nseg, nullptr, dp,
-                                (long long)np, pl->scratch, config, cs);
-    cudaError_t e2 = cudaStreamEndCapture(cs, &pl->graph);
-    if (e == cudaSuccess) e = e2;
-  }
-  if (e == cudaSuccess && rc == B2P_OK) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
-  cudaStreamDestroy(cs);
-  if (e != cudaSuccess || rc != B2P_OK) {
-    b2p_plan_destroy(pl);
-    return rc != B2P_OK ? rc : cuda_status(e);
+    return rc;
   }
   *plan = pl;
   return B2P_OK;

@@ -19,7 +19,7 @@
 // W3 gradients, so the per-block gradient needs no atomics), a fixed-order
 // reduction of the per-block gradients (deterministic), Adam, and batched
 // inference with a masked argmax.
-#include "common.cuh"
+#include "b2p_device/common.cuh"
 #include "internal.h"
 #include "tuning.h"
 

@@ -7,7 +7,7 @@
 // work-items for reductions (util/memory_streaming.hpp:30-47,
 // algorithms/numeric.hpp:154-158) and 128 work-items x 16 items for scans
 // (algorithms/scan/scan.hpp:26-32, decoupled_lookback_scan.hpp:481-488).
-#include "common.cuh"
+#include "b2p_device/common.cuh"
 #include "internal.h"
 #include "tuning.h"
 

@@ -9,6 +9,7 @@
 // only when every check passed.
 #include <hipSYCL_b2p/stdpar.hpp>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <numeric>
@@ -532,6 +533,30 @@ static void test_stdpar() {
 // Config 2's fp32 values (seed 1) through sycl::reduction: within 1e-6 of a
 // float64 host sum.
 
+// Median time of `reps` runs of f on the queue's stream (CUDA events).
+template <class F>
+static float median_ms(sycl::queue &q, F f, int reps = 7) {
+  std::vector<float> t;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  f();
+  q.wait();
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(a, q.cuda_stream());
+    f();
+    cudaEventRecord(b, q.cuda_stream());
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    t.push_back(ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::sort(t.begin(), t.end());
+  return t[t.size() / 2];
+}
+
 static void test_workload_configs(sycl::queue &q) {
   alg::util::allocation_cache cache{alg::util::allocation_type::device};
   {
@@ -573,6 +598,27 @@ static void test_workload_configs(sycl::queue &q) {
         .wait();
     CHECK(std::fabs((double)*sum - ref) <= 1e-6 * std::fabs(ref), "fp32 sycl::reduction 2^28 got %.9g want %.9g",
           (double)*sum, ref);
+    // the same sum through hipsycl::algorithms::reduce (libb2p's b2p_reduce)
+    // and through a user transform
+    float *r2 = sycl::malloc_shared<float>(1, q);
+    {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      alg::reduce(q, g, d, d + n, r2, 0.f, sycl::plus<float>{}).wait();
+      CHECK(std::fabs((double)*r2 - ref) <= 1e-6 * std::fabs(ref), "fp32 algorithms::reduce 2^28");
+      alg::transform_reduce(q, g, d, d + n, r2, 0.f, sycl::plus<float>{},
+                            [] __host__ __device__(float v) { return 2.f * v; })
+          .wait();
+      CHECK(std::fabs((double)*r2 - 2.0 * ref) <= 2e-6 * std::fabs(ref), "fp32 transform_reduce(2x) 2^28");
+      const float t_red = median_ms(q, [&] {
+        q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<float>{}),
+                       [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; });
+      });
+      const float t_lib = median_ms(q, [&] { alg::reduce(q, g, d, d + n, r2, 0.f, sycl::plus<float>{}); });
+      std::printf("TIMING fp32 2^28 sum: sycl::reduction %.4f ms, b2p_reduce %.4f ms, ratio %.3f\n", t_red, t_lib,
+                  t_red / t_lib);
+      CHECK(t_red <= 1.25f * t_lib, "sycl::reduction 2^28 within 25%% of b2p_reduce (%.4f vs %.4f ms)", t_red, t_lib);
+    }
+    sycl::free(r2, q);
     sycl::free(sum, q);
     sycl::free(d, q);
   }
@@ -595,6 +641,18 @@ static void test_workload_configs(sycl::queue &q) {
     CHECK(*cnt == ref.size(), "config 3 lambda copy_if count %zu want %zu", *cnt, ref.size());
     std::vector<uint32_t> got = from_dev(q, out, ref.size());
     CHECK(got == ref, "config 3 lambda copy_if values");
+    {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      auto lam = [] __host__ __device__(uint32_t v) { return (v & 7u) < 3u; };
+      const alg::mask_compare<uint32_t> mc{7u, 3u, B2P_CMP_LT};
+      const float t_lam = median_ms(q, [&] { alg::copy_if(q, g, d, d + n, out, lam, cnt); });
+      const float t_lib = median_ms(q, [&] { alg::copy_if(q, g, d, d + n, out, mc, cnt); });
+      std::printf("TIMING u32 2^28 copy_if: lambda %.4f ms, b2p_copy_if %.4f ms, ratio %.3f\n", t_lam, t_lib,
+                  t_lam / t_lib);
+      CHECK(t_lam <= 1.25f * t_lib, "lambda copy_if 2^28 within 25%% of b2p_copy_if (%.4f vs %.4f ms)", t_lam, t_lib);
+      q.wait();
+      CHECK(*cnt == ref.size(), "copy_if count after timing");
+    }
     sycl::free(cnt, q);
     sycl::free(out, q);
     sycl::free(d, q);

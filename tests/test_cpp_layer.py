@@ -23,6 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 def build_program() -> str:
     deps = [SRC] + glob.glob(os.path.join(ROOT, "include", "hipSYCL_b2p", "*.hpp")) + \
+        glob.glob(os.path.join(ROOT, "include", "b2p_device", "*.cuh")) + \
         [os.path.join(ROOT, "include", "b2p.h")]
     if not os.path.exists(os.path.join(LIBDIR, "libb2p.so")):
         from opensycl_b200 import build
@@ -47,4 +48,7 @@ def test_cpp_layer_builds():
 def test_cpp_layer_runs_on_gpu(dev):
     exe = build_program()
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    for line in r.stdout.splitlines():
+        if line.startswith("TIMING"):
+            print(line)
     assert r.returncode == 0 and "ALL PASSED" in r.stdout, r.stdout[-4000:] + r.stderr[-2000:]
