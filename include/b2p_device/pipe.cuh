@@ -115,6 +115,10 @@ struct PipeState {
   uint32_t tmem_base;
   unsigned long long agg[kMaxStages], carry[kMaxStages];
   int sflags[kMaxStages];  // segmented: head / carry flags of the slot's tile
+  // segmented reduce: the tile-local value and index of the segment that
+  // needs the tile's carry (the tile's first segment, ending in the tile)
+  unsigned long long local[kMaxStages];
+  long long lseg[kMaxStages];
   unsigned long long epoch;
   long long end_item;  // number of tiles this block handles, once the reducers know it
 };
@@ -334,11 +338,13 @@ __device__ __forceinline__ void pipe_init(PipeState &ps, const TmaParams &p) {
 // completes its stage without a row copy.  Tile id -1 ends the reducers.
 // The next tile id is fetched while the current one is issued, so the
 // counter's round trip overlaps the stage wait; ids stay in order per
-// block, and every id a block holds is loaded as soon as it has a stage.
+// block, and every id a block holds is loaded as soon as it has a stage (a
+// block only ever waits for tiles of lower ids, so every wait ends).
+// `end_markers` consumer groups take items in turn; each gets an end marker.
 __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaParams &p, PipeState &ps,
                                               char *smem, int rows, int box, long long *tiles,
                                               const char *rec_g = nullptr, char *rec_s = nullptr,
-                                              unsigned rec_bytes = 0) {
+                                              unsigned rec_bytes = 0, int end_markers = 1) {
   prefetch_tensormap(tin);
   const unsigned long long pol = l2_policy_stream();
   const int S = p.stages;
@@ -355,6 +361,7 @@ __device__ __forceinline__ void producer_loop(const CUtensorMap *tin, const TmaP
     if (tile >= p.ntiles) {
       tiles[s] = -1;
       mbar_arrive(&ps.full[s]);
+      if (--end_markers > 0) continue;
       return;
     }
     next = (long long)atomicAdd(&p.hdr->tile_ctr, 1ull);
@@ -421,9 +428,10 @@ __device__ __forceinline__ void lookback_loop(const TmaParams &p, PipeState &ps,
 __device__ __forceinline__ int emitter_wait(const TmaParams &p, PipeState &ps, const RingPos &r, long long it) {
   uint64_t t0 = 0;
   for (unsigned k = 0;; ++k) {
-    if (mbar_try(&ps.cready[r.s], r.ph)) return 1;
+    // parked up to 2 us per try: the end of the items is seen within that
+    if (mbar_try_hint(&ps.cready[r.s], r.ph, 2000)) return 1;
     if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) return 0;
-    if ((k & 31) == 31) {
+    if ((k & 7) == 7) {
       const uint64_t now = globaltimer_ns();
       if (t0 == 0) t0 = now;
       else if (now - t0 > p.timeout_ns) return -1;

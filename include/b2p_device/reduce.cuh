@@ -402,7 +402,7 @@ inline size_t reduce_gen_scratch_bytes(unsigned long long n) {
 // op(*out, total) when init is null (the policy's own rule when it has one).
 // scratch: libb2p scratch (zero-filled once, 256-byte aligned) of at least
 // reduce_gen_scratch_bytes(n).  Asynchronous on st.
-template <class P, class Src, int UNROLL = 8>
+template <class P, class Src, int UNROLL = (sizeof(typename P::In) <= 4 ? 16 : 8)>
 int launch_reduce_gen(const Src &src, unsigned long long n, void *out, const void *init, void *scratch,
                       size_t scratch_bytes, cudaStream_t st) {
   if (n == 0) return B2P_OK;

@@ -56,20 +56,34 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, unsigned parity) {
   return ok != 0;
 }
 
+// try_wait with a suspend-time hint: the thread is parked (issues nothing)
+// until the phase completes or about `hint_ns` pass.  Waiting warps of the
+// pipelined kernels share their SM sub-partitions with the warps doing the
+// work; a wait that spins on try_wait without the hint takes issue slots
+// from them.
+__device__ __forceinline__ bool mbar_try_hint(uint64_t *b, unsigned parity, unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for the phase with the given parity to complete; false after
-// timeout_ns without completion.  try_wait suspends the thread for a while
-// by itself; the clock (a slow special-register read) is looked at only
-// every 32 polls, so that hundreds of waiting threads do not crowd the
-// pipe that the working threads need.
+// timeout_ns without completion.  Each try_wait parks the thread for up to
+// 100 us (it resumes as soon as the phase completes); the clock is read
+// between tries.
+constexpr unsigned kWaitHintNs = 100000;
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity, unsigned long long timeout_ns) {
   uint64_t t0 = 0;
-  for (unsigned k = 0;; ++k) {
-    if (mbar_try(b, parity)) return true;
-    if ((k & 31) == 31) {
-      const uint64_t now = globaltimer_ns();
-      if (t0 == 0) t0 = now;
-      else if (now - t0 > timeout_ns) return false;
-    }
+  for (;;) {
+    if (mbar_try_hint(b, parity, kWaitHintNs)) return true;
+    const uint64_t now = globaltimer_ns();
+    if (t0 == 0) t0 = now;
+    else if (now - t0 > timeout_ns) return false;
   }
 }
 

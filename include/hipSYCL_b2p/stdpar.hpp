@@ -25,11 +25,20 @@
 // Offload front (offload.hpp:165-238, detail/stdpar_builtins.hpp:17-37):
 // managed (shared-USM) ranges are prefetched to the GPU on the call's stream
 // before the kernel; the policy b2p_stdpar::par_unseq_async leaves scans
-// non-blocking, as the reference's are, when no range needs staging: calls
-// queue back to back on the thread's in-order stream and
-// b2p_stdpar::sync() is the barrier the reference's compiler inserts before
-// host code reads the results.  reduce, transform_reduce and copy_if return
-// values and always block.
+// non-blocking, as the reference's are, when no range needs staging.
+// Consecutive non-blocking calls form one batch: the thread's queue stream
+// records them into a CUDA graph (stream capture) instead of launching them,
+// and the batch is finalised -- the graph launched once -- at
+// b2p_stdpar::sync(), the barrier the reference's compiler inserts before
+// host code reads the results, or at the next blocking call, which must run
+// after the batch (the reference counts outstanding operations and
+// finalises its batch at that barrier: stdpar_builtins.hpp:17-37,
+// detail/sycl_glue.hpp:120-139, offload.hpp:597-683).  A batch of the same
+// shape as the previous one updates the previous executable graph instead
+// of instantiating a new one.  Ranges of calls inside a batch are not
+// prefetched (the hint is not part of the graph).  reduce,
+// transform_reduce, copy_if and any/all/none_of return values and always
+// block.
 #pragma once
 
 #include "algorithms.hpp"
@@ -62,9 +71,60 @@ struct tls_runtime {
   b2p_sycl::queue q;
   alg::util::allocation_cache cache{alg::util::allocation_type::device};
   std::vector<offload_record> history;
+  // the open batch of non-blocking calls (stream capture of q's stream)
+  bool capturing = false;
+  size_t batch_calls = 0;
+  cudaGraphExec_t exec = nullptr;
+  size_t graph_launches = 0, batched_calls = 0;
+
   static tls_runtime &get() {
     thread_local tls_runtime rt;
     return rt;
+  }
+  ~tls_runtime() {
+    try {
+      flush();
+    } catch (...) {
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGetLastError();
+  }
+  // Start recording the thread's calls into a batch (if none is open).
+  void begin_batch() {
+    if (capturing) return;
+    b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+    b2p_sycl::detail::check_cuda(cudaStreamBeginCapture(q.cuda_stream(), cudaStreamCaptureModeRelaxed),
+                                 "stdpar batch: begin capture");
+    capturing = true;
+    batch_calls = 0;
+  }
+  // Finalise the open batch: end the capture and launch its graph once on
+  // the queue (asynchronously).  Nothing to do without an open batch.
+  void flush() {
+    if (!capturing) return;
+    capturing = false;
+    b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+    cudaGraph_t graph = nullptr;
+    b2p_sycl::detail::check_cuda(cudaStreamEndCapture(q.cuda_stream(), &graph), "stdpar batch: end capture");
+    if (batch_calls > 0 && graph) {
+      if (exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(exec, graph, &info) != cudaSuccess) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(exec);
+          exec = nullptr;
+        }
+      }
+      cudaError_t e = exec ? cudaSuccess : cudaGraphInstantiate(&exec, graph, 0);
+      if (e == cudaSuccess) e = cudaGraphLaunch(exec, q.cuda_stream());
+      cudaGraphDestroy(graph);
+      b2p_sycl::detail::check_cuda(e, "stdpar batch: launch");
+      ++graph_launches;
+      batched_calls += batch_calls;
+    } else if (graph) {
+      cudaGraphDestroy(graph);
+    }
+    batch_calls = 0;
   }
 };
 
@@ -91,7 +151,7 @@ class view {
       : host_(p), n_(n), rt_(rt) {
     if (alg::detail::device_accessible(p)) {
       dev_ = p;
-      if (n && is_managed(p)) {  // pages move to the GPU ahead of the kernel
+      if (n && !rt.capturing && is_managed(p)) {  // pages move to the GPU ahead of the kernel
         int dev = 0;
         cudaGetDevice(&dev);
         if (cudaMemPrefetchAsync(p, n * sizeof(T), dev, rt.q.cuda_stream()) != cudaSuccess) cudaGetLastError();
@@ -133,6 +193,7 @@ template <class T, class F>
 T reduce_impl(const char *name, size_t n, F &&launch) {
   timer tm(name, n);
   auto &rt = tls_runtime::get();
+  rt.flush();  // after the calls of the open batch
   alg::util::allocation_group g(&rt.cache, rt.q.get_device());
   T *d_out = g.obtain<T>(1);
   launch(g, rt, d_out);
@@ -148,9 +209,25 @@ T reduce_impl(const char *name, size_t n, F &&launch) {
 // non-blocking scans, the time to enqueue).
 inline const std::vector<offload_record> &offload_history() { return detail::tls_runtime::get().history; }
 
-// Wait for every call this thread has offloaded (the barrier before host
-// code reads the results of par_unseq_async scans).
-inline void sync() { detail::tls_runtime::get().q.wait(); }
+// Finalise the open batch and wait for every call this thread has
+// offloaded (the barrier before host code reads the results of
+// par_unseq_async scans).
+inline void sync() {
+  auto &rt = detail::tls_runtime::get();
+  rt.flush();
+  rt.q.wait();
+}
+
+// Batches of non-blocking calls finalised so far on this thread: graphs
+// launched, and calls they held.
+struct batch_stats_t {
+  size_t graph_launches;
+  size_t batched_calls;
+};
+inline batch_stats_t batch_stats() {
+  auto &rt = detail::tls_runtime::get();
+  return {rt.graph_launches, rt.batched_calls};
+}
 
 }  // namespace b2p_stdpar
 
@@ -229,14 +306,34 @@ OutputIt scan_call(const b2p_stdpar::par_unseq_policy &pol, const char *name, In
   if (n == 0) return d_first;
   d::timer tm(name, n);
   auto &rt = d::tls_runtime::get();
+  // a non-blocking scan over ranges the GPU reaches joins the open batch;
+  // any other call finalises it first
+  const bool batch = pol.nonblocking_scans && hipsycl::algorithms::detail::device_accessible(d::raw(first)) &&
+                     hipsycl::algorithms::detail::device_accessible(d::raw(d_first));
+  if (batch) rt.begin_batch();
+  else rt.flush();
   hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
   using V = typename std::iterator_traits<InputIt>::value_type;
   using O = std::remove_reference_t<decltype(*d_first)>;
   d::view<const V> in(g, rt, d::raw(first), n, true);
   d::view<O> out(g, rt, d::raw(d_first), n, false);
+  if (batch) {
+    try {
+      run(rt.q, g, in.get(), in.get() + n, out.get());
+    } catch (...) {
+      rt.batch_calls = 0;
+      try {
+        rt.flush();  // ends the failed capture and drops its graph
+      } catch (...) {
+      }
+      throw;
+    }
+    ++rt.batch_calls;
+    return d_first + n;
+  }
   run(rt.q, g, in.get(), in.get() + n, out.get());
   out.copy_back(n);
-  if (!pol.nonblocking_scans || in.staged() || out.staged()) rt.q.wait();
+  rt.q.wait();
   return d_first + n;
 }
 }  // namespace b2p_stdpar_detail
@@ -328,6 +425,7 @@ bool flag_call(const char *name, ForwardIt first, ForwardIt last, bool empty_ans
   if (n == 0) return empty_answer;
   d::timer tm(name, n);
   auto &rt = d::tls_runtime::get();
+  rt.flush();
   hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
   using V = typename std::iterator_traits<ForwardIt>::value_type;
   d::view<const V> in(g, rt, d::raw(first), n, true);
@@ -371,6 +469,7 @@ ForwardIt2 copy_if(const b2p_stdpar::par_unseq_policy &, ForwardIt1 first, Forwa
   if (n == 0) return d_first;
   d::timer tm("copy_if", n);
   auto &rt = d::tls_runtime::get();
+  rt.flush();
   hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
   using V = typename std::iterator_traits<ForwardIt1>::value_type;
   using O = std::remove_reference_t<decltype(*d_first)>;

@@ -43,7 +43,6 @@ constexpr int kSegHasHead = 1;
 constexpr int kSegNeedCarry = 2;  // some output of the tile needs the carry
 // per-thread word from reducers to emitters
 constexpr unsigned long long kSegTexclF = 1ull << 63;  // the thread's exclusive prefix has a head
-constexpr unsigned long long kSegHasEnd = 1ull << 62;  // reduce: the entering segment ends here
 
 // Boundary i of the tile, relative to the tile's first element (the staged
 // record, or global memory when the tile has more than a record holds).
@@ -65,8 +64,15 @@ struct SegBounds {
   }
 };
 
+// Reducer groups of a reduce (the reduce needs no emitters): as many as fit
+// in 1024 threads beside the look-back, producer and store warps.
+constexpr int seg_groups(int nc, bool reduce) { return reduce ? (nc <= 128 ? 4 : 3) : 1; }
+constexpr int seg_threads(int nc, bool reduce) {
+  return reduce ? seg_groups(nc, true) * nc + 32 * kLookWarps + 64 : pipe_threads(nc);
+}
+
 template <class P, int NC, int ITEMS, bool WIDE, bool REDUCE>
-__global__ void __launch_bounds__(pipe_threads(NC), 1)
+__global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
     seg_tmem_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
                     TmaParams p) {
   using In = typename P::In;
@@ -85,6 +91,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   static_assert(kCols == 16 || kCols == 32, "TMEM columns per thread");
   static_assert(NC % 128 == 0, "reducer and emitter groups cover the four TMEM lane quarters evenly");
   static_assert(ITEMS <= 32, "head mask is 32 bits");
+  // look-back warps of a reduce (its emitter places hold the second group)
+  constexpr int kSegLookWarps = kLookWarps;
   constexpr int kSlotCols = kCols * (NC / 128);
 
   extern __shared__ char smem_raw[];
@@ -92,15 +100,30 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   char *obase = smem + p.out_base;
   Acc *texcl_all = reinterpret_cast<Acc *>(smem + p.texcl_base);
   unsigned long long *info_all = reinterpret_cast<unsigned long long *>(smem + p.info_base);
-  Acc *rend_all = reinterpret_cast<Acc *>(smem + p.rend_base);
   __shared__ __align__(8) PipeState ps;
-  __shared__ Pair s_warp[32];
-  __shared__ int s_go[2];
-  __shared__ int s_entering_end;  // reduce: a thread of the tile ends the tile's first segment
+  // A reduce has several reducer groups taking items in turn (it has no
+  // emitters); a scan has one.  Per group: the leader's verdict,
+  // the group scan's warp values, and whether a thread ends the tile's first
+  // segment (reduce).
+  constexpr int kGroups = seg_groups(NC, REDUCE);
+  // warps before the look-back warps: the reducer groups (a reduce) or the
+  // reducer and emitter groups (a scan)
+  constexpr int kWorkWarps = REDUCE ? kGroups * NC / 32 : 2 * NC / 32;
+  __shared__ Pair s_warp_g[kGroups][32];
+  __shared__ Acc s_acc_g[kGroups][32];  // clean tiles: warp totals (reduce) or the scan's warp values
+  __shared__ int s_go[kGroups > 2 ? kGroups : 2];  // [g]: reducer group g; [1] of a scan: the emitters
+  __shared__ int s_entering_end_g[kGroups];
+  __shared__ long long s_stop[kGroups];  // reduce: the item at which each group met the end
 
   const int warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_entering_end = 0;
+  if (threadIdx.x < kGroups) s_entering_end_g[threadIdx.x] = 0;
+  // a reduce hands slots back from one look-back lane, a scan from every
+  // emitter warp
   tmem_pipe_init(ps, p, NC / 32);
+  if (REDUCE && threadIdx.x == 0) {
+    for (int i = 0; i < p.slots; ++i) mbar_init(&ps.slot_free[i], 1);
+    mbar_init_fence();
+  }
   if constexpr (!REDUCE) {
     if (warp == 0) {
       __syncwarp();
@@ -114,6 +137,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   const unsigned long long epoch = ps.epoch;
   const unsigned long long epoch_tag = epoch << 8;
   const int SI = p.stages, SL = p.slots, SO = p.out_stages;
+  if (REDUCE && SL < kSegLookWarps) return;  // the host gives a reduce kMaxStages slots
   const long long last = p.ntiles - 1;
   const int ntail = (int)(p.n - p.tail_begin);
   const int ntail_out = (int)(p.n - p.tail_out_begin);
@@ -121,27 +145,40 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   // segment start value: init, or the identity
   const Acc init_acc = p.has_init ? P::from_out(from_bits64<Out>(p.init_raw)) : P::identity();
 
-  if (warp < NC / 32) {
+  if (warp < kGroups * NC / 32) {
     // ------------------------------------------------------------ reducers
-    const int t = threadIdx.x;
+    // group g takes items g, g + kGroups, ...
+    const int g = warp / (NC / 32);
+    const int t = threadIdx.x - g * NC;
+    const int gbar = 1 + g;
+    Pair *s_warp = s_warp_g[g];
+    Acc *s_acc = s_acc_g[g];
+    int &s_entering_end = s_entering_end_g[g];
     const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * kCols);
-    long long it = 0;
+    long long it = g;
     RingPos ri, rs;
-    for (;; ++it, ri.advance(1, SI), rs.advance(1, SL)) {
+    ri.advance(g, SI);
+    rs.advance(g, SL);
+    for (;; it += kGroups, ri.advance(kGroups, SI), rs.advance(kGroups, SL)) {
       if (t == 0) {
         int go = mbar_wait(&ps.full[ri.s], ri.ph, p.timeout_ns) ? 1 : -1;
         if (go > 0 && ps.tile_in[ri.s] < 0) go = 0;
         if (go > 0 && !mbar_wait(&ps.slot_free[rs.s], rs.ph ^ 1u, p.timeout_ns)) go = -1;
         if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
-        s_go[0] = go;
+        s_go[g] = go;
       }
-      bar_named(1, NC);
-      if (s_go[0] <= 0) break;
+      bar_named(gbar, NC);
+      if (s_go[g] <= 0) break;
       (void)mbar_try(&ps.full[ri.s], ri.ph);  // completed: this thread's acquire of the TMA bytes
       if constexpr (!REDUCE) tmem_fence_after();
       const long long tile = ps.tile_in[ri.s];
       char *buf = smem + (size_t)ri.s * p.stage_stride;
-      if (tile == last && ntail > 0) load_row_tail<In, NC>(p, buf, tile, kTile);
+      if (tile == last && ntail > 0) {
+        // elements past the complete rows (only in the last tile)
+        const long long j0 = (long long)p.tail_begin - tile * kTile;
+        if (t < ntail) *smem_elem_ptr<In>(buf, (int)j0 + t) = reinterpret_cast<const In *>(p.in)[p.tail_begin + t];
+        bar_named(gbar, NC);
+      }
       const long long T0 = tile * kTile;
       const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)T0);
       // the tile's boundaries plus the first one after it, from the tile's
@@ -185,8 +222,38 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       Acc r_end = P::identity();
       uint32_t w[kCols];
       constexpr int IPV = 16 / (int)sizeof(In), VPT = ITEMS / IPV, WPO = (int)sizeof(Out) / 4;
-      if (heads == 0 && (!REDUCE || ends == 0)) {
-        // no segment starts or ends here (the common case inside long segments)
+      // A clean tile has no segment boundary inside it (a reduce: none at
+      // positions 0 .. count, a scan: no head before count); every tile
+      // inside a long segment is clean.  It needs no segmented operator:
+      // its aggregate is the plain combination of the thread totals.
+      const bool clean = m >= 1 && (REDUCE ? B.at(0) > count : B.at(0) >= count);
+      if (REDUCE && heads == 0 && ends == 0) {
+        // a reduce, no segment starts or ends here: only the thread total
+        // matters, folded in kChains independent chains (element j to chain
+        // j % kChains) so that the dependent additions overlap
+        constexpr int kChains = P::kCompensated ? 4 : 1;
+        Acc ch[kChains];
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) ch[c] = P::identity();
+        const bool full = lim == ITEMS;
+#pragma unroll
+        for (int k = 0; k < VPT; ++k) {
+          const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+          const In *ev = reinterpret_cast<const In *>(&u);
+#pragma unroll
+          for (int q = 0; q < IPV; ++q) {
+            const int j = k * IPV + q;
+            if (full || j < lim) P::add(ch[j % kChains], ev[q]);
+          }
+        }
+        if constexpr (kChains == 4) {
+          ch[0] = P::combine(ch[0], ch[1]);
+          ch[2] = P::combine(ch[2], ch[3]);
+          ch[0] = P::combine(ch[0], ch[2]);
+        }
+        run = ch[0];
+      } else if (heads == 0 && !REDUCE) {
+        // a scan, no segment starts here (the common case inside long segments)
 #pragma unroll
         for (int k = 0; k < VPT; ++k) {
           const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
@@ -279,21 +346,60 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         tmem_st16(ta, w);
         if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
       }
-      if (REDUCE && j_end >= 0) s_entering_end = 1;
+      if (clean) {
+        Acc tile_tot;
+        if constexpr (REDUCE) {
+          const Acc wt = warp_allreduce<P>(run);
+          if ((t & 31) == 0) s_acc[t >> 5] = wt;
+          bar_named(gbar, NC);
+          tile_tot = s_acc[0];
+#pragma unroll
+          for (int w = 1; w < NC / 32; ++w) tile_tot = P::combine(tile_tot, s_acc[w]);
+        } else {
+          const Acc tex = group_exclusive_scan_1bar<AccOps<P>, NC>(run, s_acc, &tile_tot, t, gbar);
+          texcl_all[(size_t)rs.s * NC + t] = tex;
+          info_all[(size_t)rs.s * NC + t] = 0ull;
+        }
+        if (t == 0) {
+          const unsigned long long bits = publish_value<P, WIDE>(tile_tot);
+          if (tile != p.stall_tile) st_status(p.status + tile, bits, epoch_tag | kFlagAgg);
+          ps.tile[rs.s] = tile;
+          ps.agg[rs.s] = bits;
+          ps.sflags[rs.s] = REDUCE ? 0 : kSegNeedCarry;
+          mbar_arrive(&ps.aggr[rs.s]);
+        }
+        if constexpr (!REDUCE) {
+          tmem_wait_st();
+          tmem_fence_before();
+        }
+        __syncwarp();
+        if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);
+        continue;
+      }
       Pair tile_agg;
-      const Pair tex = group_exclusive_scan_1bar<SegOps<P>, NC>(Pair{run, f}, s_warp, &tile_agg, t, 1);
-      texcl_all[(size_t)rs.s * NC + t] = tex.v;
-      unsigned long long info = tex.f ? kSegTexclF : 0ull;
+      const Pair tex = group_exclusive_scan_1bar<SegOps<P>, NC>(Pair{run, f}, s_warp, &tile_agg, t, gbar);
       if constexpr (REDUCE) {
+        // the segment entering this thread ends at j_end: after a head of an
+        // earlier thread of the tile its value is complete; otherwise it is
+        // the tile's first segment and needs the tile's carry, which the
+        // look-back warp adds
         if (j_end >= 0) {
           if constexpr (P::kCompensated) r_end = df_norm(r_end);
-          info |= kSegHasEnd | ((unsigned long long)j_end << 32) | (unsigned long long)(unsigned)(kb + i0 - 1);
-          rend_all[(size_t)rs.s * NC + t] = r_end;
+          const Acc v = P::combine(tex.v, r_end);
+          const long long sg = (long long)kb + i0 - 1;
+          if (tex.f) {
+            out[sg] = P::finalize(v);
+          } else {
+            ps.local[rs.s] = P::pack(v);
+            ps.lseg[rs.s] = sg;
+            s_entering_end = 1;
+          }
         }
+        bar_named(gbar, NC);  // the tile's value needing the carry is in place
       } else {
-        info |= heads;
+        texcl_all[(size_t)rs.s * NC + t] = tex.v;
+        info_all[(size_t)rs.s * NC + t] = (tex.f ? kSegTexclF : 0ull) | heads;
       }
-      info_all[(size_t)rs.s * NC + t] = info;
       if (t == 0) {
         // a scan needs the carry unless the tile starts with a head; a reduce
         // only when the tile's first segment ends in it (the others end in
@@ -319,8 +425,57 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       __syncwarp();
       if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);  // this warp's slot columns and words
     }
-    if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
-  } else if (warp < 2 * NC / 32) {
+    if constexpr (REDUCE) {
+      // both groups stopped: the item count is the lower of their end items;
+      // wake every look-back warp on the items after the last (end ..
+      // end + kSegLookWarps - 1, one per warp), each slot once its previous
+      // item is done
+      if (t == 0) s_stop[g] = it;
+      bar_named(kGroups + 1, kGroups * NC);
+      if (threadIdx.x == 0) {
+        long long end = s_stop[0];
+        for (int q = 1; q < kGroups; ++q) end = min(end, s_stop[q]);
+        *reinterpret_cast<volatile long long *>(&ps.end_item) = end;
+        RingPos r;
+        r.advance((int)(end % SL), SL);
+        // the phase parity of slot (end % SL) for item `end`
+        if ((end / SL) & 1) r.ph ^= 1u;
+        for (int j = 0; j < kSegLookWarps; ++j, r.advance(1, SL)) {
+          if (!mbar_wait(&ps.slot_free[r.s], r.ph ^ 1u, p.timeout_ns)) record_error(p.hdr, B2P_ERR_TIMEOUT);
+          mbar_arrive(&ps.aggr[r.s]);
+        }
+      }
+    } else if (t == 0) {
+      *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
+    }
+  } else if (REDUCE && warp < kWorkWarps + kLookWarps) {
+    // ----------------------------------------- look-back warps of a reduce
+    // item wi, wi + kSegLookWarps, ...
+    const int wi = warp - kWorkWarps;
+    const int lane = threadIdx.x & 31;
+    RingPos r;
+    r.advance(wi, SL);
+    for (long long it = wi;; it += kSegLookWarps, r.advance(kSegLookWarps, SL)) {
+      const int s = r.s;
+      const bool ok = __shfl_sync(0xffffffffu, (int)mbar_wait(&ps.aggr[s], r.ph, p.timeout_ns), 0) != 0;
+      if (!ok) {
+        if (lane == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
+        break;
+      }
+      if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+      const long long tile = ps.tile[s];
+      if (tile > 0 && (ps.sflags[s] & kSegNeedCarry)) {
+        bool err;
+        const typename Ops::Pub carry = lookback<Ops, false>(p.status, tile, epoch_tag, p.timeout_ns, err);
+        if (lane == 0) {
+          if (err) record_error(p.hdr, B2P_ERR_TIMEOUT);
+          out[ps.lseg[s]] = P::finalize(start_value<P, WIDE>(Ops::pack(carry), P::unpack(ps.local[s])));
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ps.slot_free[s]);
+    }
+  } else if (!REDUCE && warp < 2 * NC / 32) {
     // ------------------------------------------------------------ emitters
     const int t = threadIdx.x - NC;
     const uint32_t tcol = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(((t >> 5) >> 2) * kCols);
@@ -344,14 +499,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       const unsigned long long info = info_all[(size_t)rs.s * NC + t];
       const Acc tex = texcl_all[(size_t)rs.s * NC + t];
       const Acc start = (info & kSegTexclF) ? tex : start_value<P, WIDE>(ps.carry[rs.s], tex);
-      if constexpr (REDUCE) {
-        const bool has_end = (info & kSegHasEnd) != 0;
-        const Acc r = rend_all[(size_t)rs.s * NC + t];
-        __syncwarp();
-        if ((t & 31) == 0) mbar_arrive(&ps.slot_free[rs.s]);  // slot words and carry read
-        if (has_end) out[(long long)(unsigned)(info & 0xffffffffull)] = P::finalize(P::combine(start, r));
-        (void)tile;
-      } else {
+      if constexpr (!REDUCE) {
         tmem_fence_after();
         uint32_t w[kCols];
         const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
@@ -392,7 +540,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         }
       }
     }
-  } else if (warp < 2 * NC / 32 + kLookWarps) {
+  } else if (!REDUCE && warp < 2 * NC / 32 + kLookWarps) {
     // ------------------------------------------------------ look-back warps
     const int wi = warp - 2 * NC / 32;
     const int lane = threadIdx.x & 31;
@@ -425,10 +573,10 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       }
       __syncwarp();
     }
-  } else if (warp == 2 * NC / 32 + kLookWarps) {
+  } else if (warp == kWorkWarps + kLookWarps) {
     if ((threadIdx.x & 31) == 0)
       producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile_in, reinterpret_cast<const char *>(p.seg_rec),
-                    smem + p.rec_base, (unsigned)(kSegRecInts * sizeof(int)));
+                    smem + p.rec_base, (unsigned)(kSegRecInts * sizeof(int)), kGroups);
   } else if constexpr (!REDUCE) {
     // ---------------------------------------------------------- store warp
     if ((threadIdx.x & 31) == 0) {
@@ -476,11 +624,11 @@ bool seg_layout(TmaParams &p, int block, int items) {
   const int cols = items * (int)eo / 4;
   if (cols != 16 && cols != 32) return false;
   const size_t in_b = (size_t)block * items * es, out_b = REDUCE ? 0 : (size_t)block * items * eo;
-  int slots = REDUCE ? 8 : std::min(kMaxStages, 512 / (cols * block / 128));
+  int slots = REDUCE ? kMaxStages : std::min(kMaxStages, 512 / (cols * block / 128));
   const int so = REDUCE ? 1 : kScanOutStages;
   for (;; --slots) {
     if (slots < 2) return false;
-    const size_t per_slot = (size_t)block * (ea + 8 + (REDUCE ? ea : 0));
+    const size_t per_slot = REDUCE ? 0 : (size_t)block * (ea + 8);
     const size_t fixed = so * out_b + ((slots * per_slot + 1023) & ~size_t(1023));
     const size_t rec_b = kSegRecInts * sizeof(int);
     if (fixed + 4 * (in_b + rec_b) > kSmemBudget) continue;  // keep at least 4 input stages
@@ -492,9 +640,9 @@ bool seg_layout(TmaParams &p, int block, int items) {
     p.out_stage_stride = (unsigned)out_b;
     p.out_base = (unsigned)(si * in_b);
     p.texcl_base = (unsigned)(si * in_b + so * out_b);
-    p.info_base = (unsigned)(p.texcl_base + (size_t)slots * block * ea);
-    p.rend_base = (unsigned)(p.info_base + (size_t)slots * block * 8);
-    p.rec_base = (unsigned)((p.rend_base + (REDUCE ? (size_t)slots * block * ea : 0) + 15) & ~size_t(15));
+    p.info_base = (unsigned)(p.texcl_base + (REDUCE ? 0 : (size_t)slots * block * ea));
+    p.rend_base = (unsigned)(p.info_base + (REDUCE ? 0 : (size_t)slots * block * 8));
+    p.rec_base = (unsigned)((p.rend_base + 15) & ~size_t(15));
     return true;
   }
 }
@@ -512,7 +660,7 @@ int launch_seg_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &to
     const size_t smem = (size_t)p.rec_base + (size_t)p.stages * kSegRecInts * sizeof(int) + 1024;
     int rc = ensure_dynamic_smem((const void *)kfn, smem);
     if (rc) return rc;
-    const int threads = pipe_threads(NC);
+    const int threads = seg_threads(NC, REDUCE);
     if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
     const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
     kfn<<<grid, threads, smem, st>>>(tin, tout, p);

@@ -305,7 +305,23 @@ def main(argv=None):
     ap.add_argument("--dataset", default=DATASET)
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
+    ap.add_argument("--only-prims", default=None,
+                    help="collect: re-time only the rows of these primitive ids (comma separated) in the "
+                         "existing dataset, keeping the others")
     a = ap.parse_args(argv)
+    if a.step == "collect" and a.only_prims:
+        prims = {int(v) for v in a.only_prims.split(",")}
+        shapes, X, T, meta = load_dataset(a.dataset)
+        rows = [i for i, s in enumerate(shapes) if s["prim"] in prims]
+        t0 = time.time()
+        for k, i in enumerate(rows):
+            T[i] = tune(shapes[i], a.reps, seed=1000 + i)
+            if k % 50 == 0:
+                print(f"re-tuned {k}/{len(rows)}", flush=True)
+        meta = dict(meta, retuned={"prims": sorted(prims), "rows": len(rows), "seconds": time.time() - t0})
+        save_dataset(a.dataset, shapes, X, T, meta)
+        print("dataset", a.dataset, "re-tuned rows", len(rows), f"{time.time() - t0:.1f}s", flush=True)
+        return
     if a.step in ("collect", "all"):
         shapes = sample_shapes(a.shapes, seed=9)
         X = features(shapes)

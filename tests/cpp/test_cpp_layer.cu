@@ -499,6 +499,43 @@ static void test_stdpar() {
     cudaFree(o1);
     cudaFree(o2);
   }
+  // a batch: 8 consecutive non-blocking scans, each reading the previous
+  // output, recorded into one CUDA graph and launched once at sync(); the
+  // same batch again reuses the executable graph
+  {
+    const size_t n = (1u << 20) + 77;
+    const int kCalls = 8;
+    std::vector<int *> bufs(kCalls + 1, nullptr);
+    for (auto &b : bufs) CHECK(cudaMallocManaged(&b, n * sizeof(int)) == cudaSuccess, "cudaMallocManaged");
+    for (size_t i = 0; i < n; ++i) bufs[0][i] = (int)(i % 5) - 2;
+    std::vector<std::vector<int>> ref(kCalls + 1, std::vector<int>(n));
+    ref[0].assign(bufs[0], bufs[0] + n);
+    for (int c = 0; c < kCalls; ++c) {
+      if (c % 2 == 0) std::inclusive_scan(ref[c].begin(), ref[c].end(), ref[c + 1].begin());
+      else std::exclusive_scan(ref[c].begin(), ref[c].end(), ref[c + 1].begin(), c);
+    }
+    const auto &apol = b2p_stdpar::par_unseq_async;
+    for (int round = 0; round < 2; ++round) {
+      const auto before = b2p_stdpar::batch_stats();
+      for (int c = 0; c < kCalls; ++c) {
+        if (c % 2 == 0) std::inclusive_scan(apol, bufs[c], bufs[c] + n, bufs[c + 1]);
+        else std::exclusive_scan(apol, bufs[c], bufs[c] + n, bufs[c + 1], c);
+      }
+      b2p_stdpar::sync();
+      const auto after = b2p_stdpar::batch_stats();
+      CHECK(after.graph_launches == before.graph_launches + 1, "stdpar batch: one graph launch for %d calls (got %zu)",
+            kCalls, after.graph_launches - before.graph_launches);
+      CHECK(after.batched_calls == before.batched_calls + kCalls, "stdpar batch: %d calls in the graph", kCalls);
+      for (int c = 1; c <= kCalls; ++c)
+        CHECK(std::equal(ref[c].begin(), ref[c].end(), bufs[c]), "stdpar batch round %d call %d result", round, c);
+      for (int c = 1; c <= kCalls; ++c) std::fill(bufs[c], bufs[c] + n, -1);
+    }
+    // a blocking call finalises the open batch before it runs
+    std::inclusive_scan(apol, bufs[0], bufs[0] + n, bufs[1]);
+    const long long red = std::reduce(b2p_stdpar::par_unseq, bufs[1], bufs[1] + n, 0ll);
+    CHECK(red == std::accumulate(ref[1].begin(), ref[1].end(), 0ll), "stdpar reduce after a batched scan");
+    for (auto b : bufs) cudaFree(b);
+  }
   // any_of / all_of / none_of (algorithm.hpp:422-516, pstl-impl/algorithm.hpp:403-500)
   for (size_t n : {1ul, 1000ul, (1ul << 22) + 7}) {
     std::vector<int> v(n);
