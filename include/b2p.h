@@ -88,7 +88,8 @@ typedef enum b2p_prim {
   B2P_PRIM_HISTOGRAM = 3,
   B2P_PRIM_DOT = 4,
   B2P_PRIM_SEG_REDUCE = 5,
-  B2P_PRIM_SEG_SCAN = 6
+  B2P_PRIM_SEG_SCAN = 6,
+  B2P_PRIM_SORT = 7 /* scratch sizing only */
 } b2p_prim;
 
 /* copy_if predicate family: (x & mask) CMP rhs on the element's bits */
@@ -253,6 +254,28 @@ int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in,
 int b2p_segmented_per_call(int prim, int dtype, int op, const void *in, void *out,
                            const int64_t *host_offsets, int64_t nseg, void *scratch,
                            size_t scratch_bytes, int config, b2p_stream stream);
+
+/* Stable merge of the sorted ranges a[0..na) and b[0..nb) into
+ * out[0..na+nb) (ascending, or descending when descending != 0; on equal
+ * keys the elements of a come first).  dtype I32, I64, U32, U64, F32, F64;
+ * floats compare with < (NaNs unordered).  One pass: merge-path tiles.
+ * Replaces hipsycl::algorithms::merge (algorithms/algorithm.hpp:519-560,
+ * algorithms/merge/merge.hpp:222-313) for these types with std::less /
+ * std::greater. */
+int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
+              b2p_stream stream);
+
+/* Sort keys[0..n) in place, ascending (descending != 0: descending),
+ * stable.  dtype as b2p_merge.  scratch: device memory of at least
+ * b2p_scratch_bytes(B2P_PRIM_SORT, dtype, n, 0, B2P_CONFIG_AUTO) bytes (a
+ * second array of n keys; its contents need no initialisation).  The sort
+ * overwrites it with keys, so it must not be a scratch buffer that the
+ * other primitives use for their look-back status words.  A merge
+ * sort: tiles sorted in shared memory, then log2(n / tile) merge passes.
+ * Replaces hipsycl::algorithms::sort (algorithms/algorithm.hpp:519-529,
+ * algorithms/sort/bitonic_sort.hpp:69-110). */
+int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
+             b2p_stream stream);
 
 /* Wait for `stream`, then read the sticky device error word kept in
  * `scratch` (B2P_OK or B2P_ERR_TIMEOUT); clear != 0 resets it.  scratch ==

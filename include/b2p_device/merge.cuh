@@ -1,0 +1,268 @@
+// Merge and sort, shared by libb2p (b2p_merge, b2p_sort) and the
+// header-only C++ layer (hipsycl::algorithms::merge / sort and the stdpar
+// std::merge / std::sort overloads with any comparator).
+//
+// Replaces the reference's merge (algorithms/merge/merge.hpp:222-313:
+// merge-path partitioning, hierarchical hybrid merge) and sort
+// (algorithms/sort/bitonic_sort.hpp:69-110: an in-place bitonic network of
+// log2(n)^2 / 2 global passes) with:
+//   merge  one pass over the output in tiles: each block finds its tile's
+//          split of the two inputs on the merge path (binary search along
+//          the tile's first diagonal), stages both input ranges in shared
+//          memory, and every thread merges its ITEMS outputs after its own
+//          merge-path search in shared memory; outputs leave in coalesced
+//          rows.  Reads each input once, writes each output once.
+//   sort   a merge sort: blocks sort tiles in shared memory (a stable
+//          odd-even sort of each thread's ITEMS keys in registers, then
+//          log2(threads) rounds of merge-path merges of runs in shared
+//          memory), then log2(n / tile) global passes of the merge above on
+//          pairs of runs, ping-ponging between the keys and a scratch array.
+// Both are stable: on equal keys the element of the first range (the
+// earlier run) comes first, as std::merge requires.  comp(x, y) is a strict
+// weak order ("x before y").
+#pragma once
+
+#include "common.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+
+namespace b2p {
+
+constexpr int kMergeThreads = 256;
+// Keys per thread: the two shared tiles of a block stay within 32 KiB.
+template <class T>
+constexpr int merge_items() {
+  return sizeof(T) <= 8 ? 8 : (sizeof(T) <= 16 ? 4 : (sizeof(T) <= 32 ? 2 : 1));
+}
+template <class T>
+constexpr int merge_tile() {
+  return kMergeThreads * merge_items<T>();
+}
+
+// Number of elements of `a` among the first `diag` outputs of the stable
+// merge of a[0..na) and b[0..nb) (a(i), b(i) read element i): the first i
+// in [max(0, diag - nb), min(diag, na)] whose b[diag - 1 - i] is strictly
+// before a[i].
+template <class T, class Comp, class IdxA, class IdxB>
+__device__ __forceinline__ long long merge_path(IdxA a, long long na, IdxB b, long long nb, long long diag,
+                                                const Comp &comp) {
+  long long lo = diag > nb ? diag - nb : 0;
+  long long hi = diag < na ? diag : na;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    // a[mid] goes before b[diag - 1 - mid] unless b's key is strictly smaller
+    if (!comp(b(diag - 1 - mid), a(mid))) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// merge_path() by one warp: each round the 32 lanes test 32 evenly spaced
+// points of the remaining range at once and keep the gap where the answer
+// lies (a range of `span` shrinks to about span / 33 per round: 6 rounds of
+// global-memory latency for 2^28 keys instead of 28).  Every lane returns
+// the same value.
+template <class T, class Comp, class IdxA, class IdxB>
+__device__ __forceinline__ long long merge_path_warp(IdxA a, long long na, IdxB b, long long nb, long long diag,
+                                                     const Comp &comp) {
+  const int lane = threadIdx.x & 31;
+  long long lo = diag > nb ? diag - nb : 0;
+  long long hi = diag < na ? diag : na;
+  while (lo < hi) {
+    const long long span = hi - lo;
+    if (span <= 32) {
+      const bool p = lane < span && comp(b(diag - 1 - (lo + lane)), a(lo + lane));
+      const unsigned m = __ballot_sync(0xffffffffu, p);
+      return m ? lo + (__ffs(m) - 1) : hi;
+    }
+    // probes lo + span * (k + 1) / 33, k = 0..31: strictly increasing, < hi
+    const long long pk = lo + span * (lane + 1) / 33;
+    const bool p = comp(b(diag - 1 - pk), a(pk));
+    const unsigned m = __ballot_sync(0xffffffffu, p);
+    const int j = m ? __ffs(m) - 1 : 32;
+    const long long new_lo = j == 0 ? lo : lo + span * j / 33 + 1;
+    const long long new_hi = j == 32 ? hi : lo + span * (j + 1) / 33;
+    lo = new_lo;
+    hi = new_hi;
+  }
+  return lo;
+}
+
+// Serial stable merge of `count` outputs starting at a[ia], b[ib] (shared
+// memory views), into out[0..count).
+template <class T, class Comp>
+__device__ __forceinline__ void merge_serial(const T *a, int ia, int na, const T *b, int ib, int nb, T *out,
+                                             int count, const Comp &comp) {
+#pragma unroll
+  for (int k = 0; k < merge_items<T>(); ++k) {
+    if (k < count) {
+      bool take_b;
+      if (ia >= na) take_b = true;
+      else if (ib >= nb) take_b = false;
+      else take_b = comp(b[ib], a[ia]);
+      out[k] = take_b ? b[ib++] : a[ia++];
+    }
+  }
+}
+
+// Merge tile `blockIdx.x` of the pairwise merge of runs of length `run`
+// (run >= total: one pair, the merge of a[0..na) and b[0..nb) as given).
+// For the sort passes a == b == src with na = nb = n: the pair of output
+// position d is runs [2r, 2r + run) and [2r + run, 2r + 2 run), r = d / (2
+// run) * run.
+template <class T, class Comp, bool PAIRS>
+__global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long long na, const T *b, long long nb,
+                                                              T *out, long long run, Comp comp) {
+  constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
+  __shared__ T s_in[kMergeTile];
+  __shared__ T s_out[kMergeTile];
+  __shared__ long long s_split[2];
+  const long long total = PAIRS ? na : na + nb;
+  const long long d0 = (long long)blockIdx.x * kMergeTile;
+  if (d0 >= total) return;
+  // the pair this tile belongs to (PAIRS), as two ranges A, B
+  const T *A = a;
+  const T *B = b;
+  long long nA = na, nB = nb, base = 0;
+  if constexpr (PAIRS) {
+    base = d0 / (2 * run) * (2 * run);
+    A = a + base;
+    nA = min(run, total - base);
+    B = a + base + nA;
+    nB = min(run, total - base - nA);
+  }
+  const long long tile_end = min(d0 + kMergeTile, total);
+  const long long l0 = d0 - base, l1 = tile_end - base;  // diagonals within the pair
+  auto ga = [&](long long i) { return A[i]; };
+  auto gb = [&](long long i) { return B[i]; };
+  // warp 0 finds where the tile starts on the merge path, warp 1 where it ends
+  if (threadIdx.x < 64) {
+    const long long sp = merge_path_warp<T>(ga, nA, gb, nB, threadIdx.x < 32 ? l0 : l1, comp);
+    if ((threadIdx.x & 31) == 0) s_split[threadIdx.x >> 5] = sp;
+  }
+  __syncthreads();
+  const long long i0 = s_split[0], i1 = s_split[1];
+  const long long j0 = l0 - i0, j1 = l1 - i1;
+  const int na_t = (int)(i1 - i0), nb_t = (int)(j1 - j0);
+  for (int k = threadIdx.x; k < na_t + nb_t; k += kMergeThreads)
+    s_in[k] = k < na_t ? A[i0 + k] : B[j0 + (k - na_t)];
+  __syncthreads();
+  const int cnt = na_t + nb_t;
+  const int dt = min((int)threadIdx.x * kMergeItems, cnt);
+  auto sa = [&](long long i) { return s_in[i]; };
+  auto sb = [&](long long i) { return s_in[na_t + i]; };
+  const int it = (int)merge_path<T>(sa, na_t, sb, nb_t, dt, comp);
+  T v[kMergeItems];
+  merge_serial(s_in, it, na_t, s_in + na_t, dt - it, nb_t, v, min(kMergeItems, cnt - dt), comp);
+#pragma unroll
+  for (int k = 0; k < kMergeItems; ++k)
+    if (dt + k < cnt) s_out[dt + k] = v[k];
+  __syncthreads();
+  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) out[d0 + k] = s_out[k];
+}
+
+// Sort tile `blockIdx.x` of keys[0..n) in place (stable).
+template <class T, class Comp>
+__global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long long n, Comp comp) {
+  constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
+  __shared__ T s_a[kMergeTile];
+  __shared__ T s_b[kMergeTile];
+  const long long t0 = (long long)blockIdx.x * kMergeTile;
+  const int cnt = (int)min((long long)kMergeTile, n - t0);
+  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) s_a[k] = keys[t0 + k];
+  __syncthreads();
+  // each thread: its ITEMS keys, sorted by odd-even transposition (stable:
+  // neighbours swap only when the right one is strictly before the left)
+  const int b0 = threadIdx.x * kMergeItems;
+  const int mine = max(0, min(kMergeItems, cnt - b0));
+  T v[kMergeItems];
+#pragma unroll
+  for (int k = 0; k < kMergeItems; ++k)
+    if (k < mine) v[k] = s_a[b0 + k];
+#pragma unroll
+  for (int r = 0; r < kMergeItems; ++r) {
+#pragma unroll
+    for (int k = r & 1; k + 1 < kMergeItems; k += 2) {
+      if (k + 1 < mine && comp(v[k + 1], v[k])) {
+        const T x = v[k];
+        v[k] = v[k + 1];
+        v[k + 1] = x;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMergeItems; ++k)
+    if (k < mine) s_a[b0 + k] = v[k];
+  __syncthreads();
+  // rounds: runs of ITEMS, 2 ITEMS, ... merged pairwise in shared memory
+  T *src = s_a, *dst = s_b;
+  for (int run = kMergeItems; run < cnt; run *= 2) {
+    const int d = b0;  // this thread's outputs [d, d + ITEMS)
+    if (d < cnt) {
+      const int pb = d / (2 * run) * (2 * run);
+      const int la = min(run, cnt - pb), lb = max(0, min(run, cnt - pb - la));
+      const T *ra = src + pb, *rb = src + pb + la;
+      auto sa = [&](long long i) { return ra[i]; };
+      auto sb = [&](long long i) { return rb[i]; };
+      const int dl = d - pb;
+      const int ia = (int)merge_path<T>(sa, la, sb, lb, dl, comp);
+      T w[kMergeItems];
+      merge_serial(ra, ia, la, rb, dl - ia, lb, w, min(kMergeItems, cnt - d), comp);
+#pragma unroll
+      for (int k = 0; k < kMergeItems; ++k)
+        if (d + k < cnt) dst[d + k] = w[k];
+    }
+    __syncthreads();
+    T *x = src;
+    src = dst;
+    dst = x;
+  }
+  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) keys[t0 + k] = src[k];
+}
+
+// ------------------------------------------------------------------ host
+
+// Stable merge of a[0..na) and b[0..nb) into out (asynchronous on st).
+template <class T, class Comp>
+int launch_merge(const T *a, size_t na, const T *b, size_t nb, T *out, const Comp &comp, cudaStream_t st) {
+  const long long total = (long long)(na + nb);
+  if (total == 0) return B2P_OK;
+  const long long tiles = (total + merge_tile<T>() - 1) / merge_tile<T>();
+  if (tiles > 0x7fffffffLL) return B2P_ERR_INVALID_ARG;
+  merge_kernel<T, Comp, false><<<(unsigned)tiles, kMergeThreads, 0, st>>>(a, (long long)na, b, (long long)nb, out,
+                                                                          total, comp);
+  return cudaGetLastError() == cudaSuccess ? B2P_OK : B2P_ERR_CUDA;
+}
+
+// Scratch a sort of n keys of T needs (a second array of n keys).
+template <class T>
+inline size_t sort_scratch_bytes(size_t n) {
+  return n * sizeof(T) + 256;
+}
+
+// Stable merge sort of keys[0..n) in place; scratch holds n keys of T.
+template <class T, class Comp>
+int launch_sort(T *keys, size_t n, const Comp &comp, void *scratch, size_t scratch_bytes, cudaStream_t st) {
+  if (n <= 1) return B2P_OK;
+  constexpr long long kMergeTile = merge_tile<T>();
+  const long long tiles = ((long long)n + kMergeTile - 1) / kMergeTile;
+  if (tiles > 0x7fffffffLL) return B2P_ERR_INVALID_ARG;
+  block_sort_kernel<T, Comp><<<(unsigned)tiles, kMergeThreads, 0, st>>>(keys, (long long)n, comp);
+  if (tiles == 1) return cudaGetLastError() == cudaSuccess ? B2P_OK : B2P_ERR_CUDA;
+  if (!scratch || scratch_bytes < n * sizeof(T)) return B2P_ERR_SCRATCH;
+  T *src = keys, *dst = reinterpret_cast<T *>(scratch);
+  for (long long run = kMergeTile; run < (long long)n; run *= 2) {
+    merge_kernel<T, Comp, true><<<(unsigned)tiles, kMergeThreads, 0, st>>>(src, (long long)n, src, 0, dst, run,
+                                                                          comp);
+    T *x = src;
+    src = dst;
+    dst = x;
+  }
+  if (src != keys && cudaMemcpyAsync(keys, src, n * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return B2P_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? B2P_OK : B2P_ERR_CUDA;
+}
+
+}  // namespace b2p

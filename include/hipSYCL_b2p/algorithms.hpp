@@ -1,7 +1,7 @@
 // Drop-in for AdaptiveCpp's algorithms library on the data-parallel
 // primitive path: hipsycl::algorithms::{reduce, transform_reduce,
 // inclusive_scan, exclusive_scan, transform_inclusive_scan,
-// transform_exclusive_scan, copy_if, any_of, all_of, none_of} and
+// transform_exclusive_scan, copy_if, any_of, all_of, none_of, sort, merge} and
 // util::{allocation_cache,
 // allocation_group}, with the reference's signatures
 // (algorithms/numeric.hpp:170-327, algorithms/algorithm.hpp:178-243,
@@ -27,6 +27,7 @@
 
 #include "sycl.hpp"
 #include "../b2p_device/copy_if.cuh"
+#include "../b2p_device/merge.cuh"
 
 #include <algorithm>
 #include <functional>
@@ -881,6 +882,141 @@ b2p_sycl::event none_of(b2p_sycl::queue &q, ForwardIt first, ForwardIt last, det
   if (first == last) return b2p_sycl::event{};
   q.depends_on(deps);
   return detail::early_exit_search(q, first, (size_t)std::distance(first, last), out, p, false, true);
+}
+
+// ------------------------------------------------------------ sort / merge
+// (algorithm.hpp:519-560).  Both are stable merge-path kernels
+// (b2p_device/merge.cuh) for any comparator callable on the device: sort is
+// a merge sort, merge one pass over the output.  Keys of the standard types
+// with std::less / std::greater on contiguous ranges go through libb2p
+// (b2p_sort, b2p_merge); other comparators and types run the same kernels
+// compiled into the caller; non-pointer iterators are gathered into a
+// contiguous buffer first and scattered back after.  The reference's sort is
+// an in-place bitonic network without scratch; this one needs a second
+// array of n keys, taken from the stream-ordered allocator of the queue's
+// stream and released in stream order.
+
+namespace detail {
+
+template <class T, class It>
+__global__ void gather_kernel(It first, size_t n, T *out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = *(first + i);
+}
+
+template <class T, class It>
+__global__ void scatter_kernel(const T *in, size_t n, It out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    *(out + i) = in[i];
+}
+
+inline unsigned copy_grid(size_t n) { return (unsigned)std::min<size_t>((n + kGB - 1) / kGB, 148 * 16); }
+
+template <class C>
+struct std_order : std::integral_constant<int, 0> {};
+template <class U>
+struct std_order<std::less<U>> : std::integral_constant<int, 1> {};
+template <class U>
+struct std_order<std::greater<U>> : std::integral_constant<int, 2> {};
+
+// dtype code of a key type libb2p sorts and merges, or -1
+template <class T>
+constexpr int sort_dtype() {
+  constexpr int d = dtype_code<T>();
+  return (d >= 0 && d != B2P_BF16) ? d : -1;
+}
+
+template <class T>
+void check_sortable() {
+  static_assert(std::is_trivially_copyable_v<T>, "sort/merge: keys must be trivially copyable");
+  static_assert(sizeof(T) <= 64, "sort/merge: keys of more than 64 bytes are not supported");
+}
+
+}  // namespace detail
+
+template <class RandomIt, class Compare = std::less<>>
+b2p_sycl::event sort(b2p_sycl::queue &q, RandomIt first, RandomIt last, Compare comp = std::less<>{},
+                     const std::vector<b2p_sycl::event> &deps = {}) {
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return b2p_sycl::event{};
+  using T = std::remove_cv_t<detail::value_t<RandomIt>>;
+  detail::check_sortable<T>();
+  q.depends_on(deps);
+  detail::require_device(first, "sort");
+  b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+  cudaStream_t st = q.cuda_stream();
+  T *keys = nullptr;
+  constexpr bool contiguous = std::is_pointer_v<RandomIt>;
+  if constexpr (contiguous) {
+    keys = const_cast<T *>(&*first);
+  } else {
+    b2p_sycl::detail::check_cuda(cudaMallocAsync((void **)&keys, n * sizeof(T), st), "sort: keys");
+    detail::gather_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(first, n, keys);
+  }
+  void *tmp = nullptr;
+  const size_t tmp_bytes = n * sizeof(T) + 256;
+  if (n > (size_t)::b2p::merge_tile<T>())
+    b2p_sycl::detail::check_cuda(cudaMallocAsync(&tmp, tmp_bytes, st), "sort: scratch");
+  int rc;
+  constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
+  if constexpr (dt >= 0 && ord != 0)
+    rc = b2p_sort(dt, keys, n, ord == 2, tmp, tmp ? tmp_bytes : 0, (b2p_stream)st);
+  else
+    rc = ::b2p::launch_sort(keys, n, comp, tmp, tmp ? tmp_bytes : 0, st);
+  if (tmp) cudaFreeAsync(tmp, st);
+  if constexpr (!contiguous) {
+    detail::scatter_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(keys, n, first);
+    cudaFreeAsync(keys, st);
+  }
+  b2p_sycl::detail::check_b2p(rc, "sort");
+  b2p_sycl::detail::check_cuda(cudaGetLastError(), "sort");
+  return q.record();
+}
+
+template <class ForwardIt1, class ForwardIt2, class ForwardIt3, class Compare = std::less<>>
+b2p_sycl::event merge(b2p_sycl::queue &q, util::allocation_group &scratch, ForwardIt1 first1, ForwardIt1 last1,
+                      ForwardIt2 first2, ForwardIt2 last2, ForwardIt3 d_first, Compare comp = std::less<>{},
+                      const std::vector<b2p_sycl::event> &deps = {}) {
+  const size_t n1 = (size_t)std::distance(first1, last1), n2 = (size_t)std::distance(first2, last2);
+  if (n1 + n2 == 0) return b2p_sycl::event{};
+  using T = std::remove_cv_t<detail::value_t<ForwardIt1>>;
+  detail::check_sortable<T>();
+  q.depends_on(deps);
+  if (n1) detail::require_device(first1, "merge");
+  if (n2) detail::require_device(first2, "merge");
+  detail::require_device(d_first, "merge");
+  b2p_sycl::detail::device_guard g(q.get_device().cuda_ordinal());
+  cudaStream_t st = q.cuda_stream();
+  // contiguous views of the inputs and the output (gathered when needed)
+  auto view_in = [&](auto first, size_t n) -> const T * {
+    using It = decltype(first);
+    if constexpr (std::is_pointer_v<It> && std::is_same_v<std::remove_cv_t<detail::value_t<It>>, T>) {
+      return n ? &*first : nullptr;
+    } else {
+      T *buf = scratch.obtain<T>(n ? n : 1);
+      if (n) detail::gather_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(first, n, buf);
+      return buf;
+    }
+  };
+  const T *a = view_in(first1, n1);
+  const T *b = view_in(first2, n2);
+  constexpr bool direct_out =
+      std::is_pointer_v<ForwardIt3> && std::is_same_v<std::remove_cv_t<detail::value_t<ForwardIt3>>, T> &&
+      !std::is_const_v<std::remove_reference_t<decltype(*d_first)>>;
+  T *out = nullptr;
+  if constexpr (direct_out) out = &*d_first;
+  else out = scratch.obtain<T>(n1 + n2);
+  int rc;
+  constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
+  if constexpr (dt >= 0 && ord != 0)
+    rc = b2p_merge(dt, a, n1, b, n2, out, ord == 2, (b2p_stream)st);
+  else
+    rc = ::b2p::launch_merge(a, n1, b, n2, out, comp, st);
+  b2p_sycl::detail::check_b2p(rc, "merge");
+  if constexpr (!direct_out)
+    detail::scatter_kernel<T><<<detail::copy_grid(n1 + n2), detail::kGB, 0, st>>>(out, n1 + n2, d_first);
+  b2p_sycl::detail::check_cuda(cudaGetLastError(), "merge");
+  return q.record();
 }
 
 }  // namespace algorithms

@@ -1,8 +1,8 @@
 // Offloaded C++ standard parallel algorithms on the primitive path:
 // std::reduce (3 overloads), std::transform_reduce (3), std::inclusive_scan
 // (3), std::exclusive_scan (2), std::transform_inclusive_scan (2),
-// std::transform_exclusive_scan (1), std::copy_if and std::any_of / all_of
-// / none_of, taking the execution
+// std::transform_exclusive_scan (1), std::copy_if, std::any_of / all_of
+// / none_of, std::sort (2) and std::merge (2), taking the execution
 // policy b2p_stdpar::par_unseq (AdaptiveCpp: the par_unseq overloads of
 // std/stdpar/pstl-impl/numeric.hpp:28-576 and pstl-impl/algorithm.hpp:150-187,
 // which its compiler pass substitutes for std::execution::par_unseq; here
@@ -38,7 +38,7 @@
 // of instantiating a new one.  Ranges of calls inside a batch are not
 // prefetched (the hint is not part of the graph).  reduce,
 // transform_reduce, copy_if and any/all/none_of return values and always
-// block.
+// block; sort and merge block too (pstl-impl/algorithm.hpp:506-606).
 #pragma once
 
 #include "algorithms.hpp"
@@ -483,6 +483,58 @@ ForwardIt2 copy_if(const b2p_stdpar::par_unseq_policy &, ForwardIt1 first, Forwa
   out.copy_back(count);
   rt.q.wait();
   return d_first + count;
+}
+
+// ------------------------------------------------------------ sort / merge
+
+template <class RandomIt, class Compare>
+void sort(const b2p_stdpar::par_unseq_policy &, RandomIt first, RandomIt last, Compare comp) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n = (size_t)std::distance(first, last);
+  if (n == 0) return;
+  d::timer tm("sort", n);
+  auto &rt = d::tls_runtime::get();
+  rt.flush();
+  hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
+  using V = typename std::iterator_traits<RandomIt>::value_type;
+  d::view<V> keys(g, rt, d::raw(first), n, true);
+  hipsycl::algorithms::sort(rt.q, keys.get(), keys.get() + n, comp);
+  keys.copy_back(n);
+  rt.q.wait();
+}
+
+template <class RandomIt>
+void sort(const b2p_stdpar::par_unseq_policy &p, RandomIt first, RandomIt last) {
+  std::sort(p, first, last, std::less<>{});
+}
+
+template <class ForwardIt1, class ForwardIt2, class ForwardIt3, class Compare>
+ForwardIt3 merge(const b2p_stdpar::par_unseq_policy &, ForwardIt1 first1, ForwardIt1 last1, ForwardIt2 first2,
+                 ForwardIt2 last2, ForwardIt3 d_first, Compare comp) {
+  namespace d = b2p_stdpar::detail;
+  const size_t n1 = (size_t)std::distance(first1, last1), n2 = (size_t)std::distance(first2, last2);
+  if (n1 + n2 == 0) return d_first;
+  d::timer tm("merge", n1 + n2);
+  auto &rt = d::tls_runtime::get();
+  rt.flush();
+  hipsycl::algorithms::util::allocation_group g(&rt.cache, rt.q.get_device());
+  using V1 = typename std::iterator_traits<ForwardIt1>::value_type;
+  using V2 = typename std::iterator_traits<ForwardIt2>::value_type;
+  using O = std::remove_reference_t<decltype(*d_first)>;
+  // an empty range may come with no element to take the address of
+  d::view<const V1> a(g, rt, n1 ? d::raw(first1) : nullptr, n1, true);
+  d::view<const V2> b(g, rt, n2 ? d::raw(first2) : nullptr, n2, true);
+  d::view<O> out(g, rt, d::raw(d_first), n1 + n2, false);
+  hipsycl::algorithms::merge(rt.q, g, a.get(), a.get() + n1, b.get(), b.get() + n2, out.get(), comp);
+  out.copy_back(n1 + n2);
+  rt.q.wait();
+  return d_first + (n1 + n2);
+}
+
+template <class ForwardIt1, class ForwardIt2, class ForwardIt3>
+ForwardIt3 merge(const b2p_stdpar::par_unseq_policy &p, ForwardIt1 first1, ForwardIt1 last1, ForwardIt2 first2,
+                 ForwardIt2 last2, ForwardIt3 d_first) {
+  return std::merge(p, first1, last1, first2, last2, d_first, std::less<>{});
 }
 
 }  // namespace std

@@ -28,7 +28,8 @@ OK, ERR_INVALID_ARG, ERR_INVALID_PTR, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ER
     ERR_NO_DEVICE, ERR_IO = range(9)
 I32, I64, U32, U64, F32, BF16, F64 = range(7)
 SUM, PROD, MIN, MAX, AND, OR, XOR = range(7)
-PRIM_REDUCE, PRIM_SCAN, PRIM_COPY_IF, PRIM_HISTOGRAM, PRIM_DOT, PRIM_SEG_REDUCE, PRIM_SEG_SCAN = range(7)
+PRIM_REDUCE, PRIM_SCAN, PRIM_COPY_IF, PRIM_HISTOGRAM, PRIM_DOT, PRIM_SEG_REDUCE, PRIM_SEG_SCAN, \
+    PRIM_SORT = range(8)
 CMP_LT, CMP_LE, CMP_EQ, CMP_NE, CMP_GE, CMP_GT = range(6)
 NUM_CONFIGS = 48
 AUTO = -1
@@ -83,6 +84,8 @@ def _declare(L):
         "b2p_scan": ([i, i, i, vp, vp, sz, vp, vp, sz, i, vp], i),
         "b2p_copy_if": ([i, vp, vp, sz, u64, i, u64, vp, vp, sz, i, vp], i),
         "b2p_histogram_u8": ([vp, sz, vp, i, i, vp], i),
+        "b2p_merge": ([i, vp, sz, vp, sz, vp, i, vp], i),
+        "b2p_sort": ([i, vp, sz, i, vp, sz, vp], i),
         "b2p_segmented_reduce": ([i, i, vp, vp, i64, vp, vp, vp, sz, i, vp], i),
         "b2p_segmented_scan": ([i, i, i, vp, vp, vp, i64, vp, vp, sz, i, vp], i),
         "b2p_segmented_per_call": ([i, i, i, vp, vp, vp, i64, vp, sz, i, vp], i),
@@ -290,6 +293,36 @@ def histogram_u8(keys, bins=None, nbins=256, config: int = AUTO, stream=None):
     check(lib().b2p_histogram_u8(keys.data_ptr(), keys.numel(), bins.data_ptr(), nbins, config,
                                  _stream(stream)), "b2p_histogram_u8")
     return bins
+
+
+def merge(a, b, out=None, descending=False, stream=None):
+    """Stable merge of two sorted 1-D tensors of one dtype (elements of `a`
+    first on equal keys), like std::merge with std::less / std::greater."""
+    torch = _torch()
+    code = dtype_code(a)
+    if dtype_code(b) != code:
+        raise ValueError("merge: a and b must have the same dtype")
+    if out is None:
+        out = torch.empty(a.numel() + b.numel(), dtype=a.dtype, device=a.device)
+    check(lib().b2p_merge(code, a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
+                          int(bool(descending)), _stream(stream)), "b2p_merge")
+    return out
+
+
+def sort_(keys, descending=False, stream=None):
+    """Stable in-place sort of a 1-D tensor, like std::stable_sort.  The
+    merge passes ping-pong through a second array of n keys: a buffer of its
+    own, not the per-stream scratch, whose look-back status words must only
+    ever hold status words."""
+    torch = _torch()
+    code = dtype_code(keys)
+    nbytes = lib().b2p_scratch_bytes(PRIM_SORT, code, keys.numel(), 0, AUTO)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    with torch.cuda.stream(s):
+        tmp = torch.empty(nbytes, dtype=torch.uint8, device=keys.device)
+    check(lib().b2p_sort(code, keys.data_ptr(), keys.numel(), int(bool(descending)), tmp.data_ptr(),
+                         nbytes, _stream(stream)), "b2p_sort")
+    return keys
 
 
 def segmented_reduce(x, offsets, op="sum", init=None, out=None, config: int = AUTO, stream=None):

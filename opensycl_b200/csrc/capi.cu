@@ -101,7 +101,9 @@ int cuda_status(cudaError_t e) { return e == cudaSuccess ? B2P_OK : B2P_ERR_CUDA
 // Device-accessibility check, mirroring the reference's stdpar pointer
 // validation (std/stdpar/detail/offload.hpp:101-123) but rejecting instead
 // of falling back to the host.
-static int check_ptr(const void *p, size_t align) {
+int check_pointer(const void *p, size_t align);
+static int check_ptr(const void *p, size_t align) { return check_pointer(p, align); }
+int check_pointer(const void *p, size_t align) {
   if (!p) return B2P_ERR_INVALID_PTR;
   if (reinterpret_cast<uintptr_t>(p) % align) return B2P_ERR_INVALID_PTR;
   cudaPointerAttributes a;
@@ -220,6 +222,8 @@ size_t b2p_scratch_bytes(int prim, int dtype, size_t n, int64_t nseg, int config
   case B2P_PRIM_SEG_REDUCE:
   case B2P_PRIM_SEG_SCAN:
     return segmented_scratch_bytes(dtype, n, nseg, config);
+  case B2P_PRIM_SORT:
+    return n * dtype_size(dtype) + 256;
   default:
     return 0;
   }

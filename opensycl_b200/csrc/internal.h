@@ -39,6 +39,10 @@ long long debug_stall_tile();
 // Record a CUDA failure; returns B2P_ERR_CUDA or B2P_OK.
 int cuda_status(cudaError_t e);
 
+// Device-accessibility and alignment check of a pointer (B2P_OK or
+// B2P_ERR_INVALID_PTR); no CPU fallback.
+int check_pointer(const void *p, size_t align);
+
 // Reduce / dot.  b == nullptr: reduce; otherwise dot.
 // Argument, device and pointer checks of b2p_reduce (B2P_OK when n == 0).
 int validate_reduce(int dtype, int op, const void *in, size_t n, const void *out);

@@ -1,0 +1,80 @@
+// b2p_merge / b2p_sort: the merge-path merge and the merge sort of
+// b2p_device/merge.cuh for the standard key types, ascending (std::less) or
+// descending (std::greater).
+#include "b2p_device/merge.cuh"
+#include "internal.h"
+
+namespace b2p {
+
+namespace {
+
+template <class T>
+struct Less {
+  __device__ __forceinline__ bool operator()(const T &x, const T &y) const { return x < y; }
+};
+template <class T>
+struct Greater {
+  __device__ __forceinline__ bool operator()(const T &x, const T &y) const { return y < x; }
+};
+
+template <class T>
+int merge_t(const void *a, size_t na, const void *b, size_t nb, void *out, bool desc, cudaStream_t st) {
+  const T *pa = reinterpret_cast<const T *>(a), *pb = reinterpret_cast<const T *>(b);
+  T *po = reinterpret_cast<T *>(out);
+  return desc ? launch_merge(pa, na, pb, nb, po, Greater<T>{}, st) : launch_merge(pa, na, pb, nb, po, Less<T>{}, st);
+}
+
+template <class T>
+int sort_t(void *keys, size_t n, bool desc, void *scratch, size_t sb, cudaStream_t st) {
+  T *k = reinterpret_cast<T *>(keys);
+  return desc ? launch_sort(k, n, Greater<T>{}, scratch, sb, st) : launch_sort(k, n, Less<T>{}, scratch, sb, st);
+}
+
+bool sortable(int dtype) { return dtype >= B2P_I32 && dtype <= B2P_F64 && dtype != B2P_BF16; }
+
+}  // namespace
+
+}  // namespace b2p
+
+using namespace b2p;
+
+extern "C" int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
+                         b2p_stream stream) {
+  if (!sortable(dtype)) return dtype == B2P_BF16 ? B2P_ERR_UNSUPPORTED : B2P_ERR_INVALID_ARG;
+  if (na + nb == 0) return B2P_OK;
+  const size_t es = dtype_size(dtype);
+  int rc;
+  if ((na && (rc = check_pointer(a, es))) || (nb && (rc = check_pointer(b, es))) || (rc = check_pointer(out, es)))
+    return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (dtype) {
+  case B2P_I32: return merge_t<int32_t>(a, na, b, nb, out, descending, st);
+  case B2P_I64: return merge_t<long long>(a, na, b, nb, out, descending, st);
+  case B2P_U32: return merge_t<uint32_t>(a, na, b, nb, out, descending, st);
+  case B2P_U64: return merge_t<unsigned long long>(a, na, b, nb, out, descending, st);
+  case B2P_F32: return merge_t<float>(a, na, b, nb, out, descending, st);
+  default: return merge_t<double>(a, na, b, nb, out, descending, st);
+  }
+}
+
+extern "C" int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
+                        b2p_stream stream) {
+  if (!sortable(dtype)) return dtype == B2P_BF16 ? B2P_ERR_UNSUPPORTED : B2P_ERR_INVALID_ARG;
+  if (n <= 1) return B2P_OK;
+  const size_t es = dtype_size(dtype);
+  int rc = check_pointer(keys, es);
+  if (rc) return rc;
+  if (n > (size_t)merge_tile<long long>()) {
+    if (!scratch || scratch_bytes < n * es) return B2P_ERR_SCRATCH;
+    if ((rc = check_pointer(scratch, es))) return B2P_ERR_SCRATCH;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (dtype) {
+  case B2P_I32: return sort_t<int32_t>(keys, n, descending, scratch, scratch_bytes, st);
+  case B2P_I64: return sort_t<long long>(keys, n, descending, scratch, scratch_bytes, st);
+  case B2P_U32: return sort_t<uint32_t>(keys, n, descending, scratch, scratch_bytes, st);
+  case B2P_U64: return sort_t<unsigned long long>(keys, n, descending, scratch, scratch_bytes, st);
+  case B2P_F32: return sort_t<float>(keys, n, descending, scratch, scratch_bytes, st);
+  default: return sort_t<double>(keys, n, descending, scratch, scratch_bytes, st);
+  }
+}

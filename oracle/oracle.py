@@ -203,3 +203,26 @@ def bf16_round(x):
 
 def bf16_to_f32(h):
     return (np.asarray(h, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def merge(a, b, descending=False):
+    """Stable merge of two sorted arrays: on equal keys the elements of `a`
+    come first (std::merge, which AdaptiveCpp's tests/pstl/merge.cpp:24-43
+    compare hipsycl::algorithms::merge against; algorithm.hpp:531-560).
+    A stable sort of a ++ b gives exactly that order."""
+    x = np.concatenate([np.asarray(a), np.asarray(b)])
+    return sort(x, descending)
+
+
+def sort(x, descending=False):
+    """Stable sort (std::stable_sort with std::less / std::greater); for keys
+    that compare equal only when identical this is also the unique result of
+    std::sort and of the reference's bitonic sort
+    (algorithms/sort/bitonic_sort.hpp:69-110), which tests/pstl/sort.cpp:24-37
+    compares against std::sort."""
+    x = np.asarray(x)
+    if not descending:
+        return x[np.argsort(x, kind="stable")]
+    # descending and stable: reverse, sort ascending stably, reverse back
+    r = x[::-1]
+    return r[np.argsort(r, kind="stable")][::-1].copy()

@@ -2,7 +2,7 @@
 // algorithms library signatures, sycl::reduction in parallel_for, group
 // algorithms, atomic_ref and the stdpar overloads.  The cases follow the
 // reference's own tests (tests/pstl/{reduce,transform_reduce,
-// inclusive_scan,exclusive_scan,copy_if}.cpp, tests/sycl/reduction.cpp,
+// inclusive_scan,exclusive_scan,copy_if,sort,merge}.cpp, tests/sycl/reduction.cpp,
 // tests/sycl/group_functions/group_functions_{reduce,scan}.cpp,
 // tests/sycl/atomic.cpp); expected values are computed here on the host.
 // Prints one line per failure and "ALL PASSED <n>" at the end; exit code 0
@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <numeric>
+#include <random>
 #include <vector>
 
 namespace alg = hipsycl::algorithms;
@@ -561,15 +562,6 @@ static void test_stdpar() {
   CHECK(!b2p_stdpar::offload_history().empty(), "stdpar offload history recorded");
 }
 
-// ----------------------------------------------- workload configurations
-// Config 1: 2^24 int32 U[-1000, 1000] (seed 0) through the entry points it
-// names -- sycl::reduction in parallel_for, std::reduce and
-// std::inclusive_scan on the stdpar policy -- bit-exact against a host sum /
-// scan.  Config 3: hipsycl::algorithms::copy_if with a lambda predicate
-// (x & 7) < 3 on 2^28 uint32 (seed 4), bit-exact and order-preserving.
-// Config 2's fp32 values (seed 1) through sycl::reduction: within 1e-6 of a
-// float64 host sum.
-
 // Median time of `reps` runs of f on the queue's stream (CUDA events).
 template <class F>
 static float median_ms(sycl::queue &q, F f, int reps = 7) {
@@ -593,6 +585,134 @@ static float median_ms(sycl::queue &q, F f, int reps = 7) {
   std::sort(t.begin(), t.end());
   return t[t.size() / 2];
 }
+
+// ------------------------------------------------------------ sort / merge
+// tests/pstl/sort.cpp:24-75 and tests/pstl/merge.cpp:24-137 through the
+// stdpar overloads (pageable std::vector ranges, staged), then the
+// algorithms-library calls with user comparators on device memory: a key
+// with a payload sorted and merged on the key alone must come out in
+// std::stable_sort / std::merge order (stability), and sizes around the
+// 2048-key tile of the kernels.
+
+struct keyed {
+  int key;
+  int idx;
+  bool operator==(const keyed &o) const { return key == o.key && idx == o.idx; }
+};
+
+static std::vector<int> sorted_random(int amount, int seed) {
+  std::mt19937 gen(seed);
+  std::uniform_int_distribution<int> dist;
+  std::vector<int> d;
+  for (int i = 0; i < amount; ++i) d.push_back(dist(gen));
+  std::sort(d.begin(), d.end());
+  return d;
+}
+
+static void test_sort_merge(sycl::queue &q) {
+  const auto &pol = b2p_stdpar::par_unseq;
+  {
+    const std::pair<size_t, int> cases[] = {{0, 0}, {1, 1}, {1024, -1}, {1024, 1}, {1000, -1}, {1000, 1}};
+    for (auto [n, sign] : cases) {
+      std::vector<int> v(n);
+      for (size_t i = 0; i < n; ++i) v[i] = sign * (int)i;
+      std::vector<int> h = v;
+      std::sort(pol, v.begin(), v.end());
+      std::sort(h.begin(), h.end());
+      CHECK(v == h && std::is_sorted(v.begin(), v.end()), "stdpar sort n=%zu sign %d", n, sign);
+    }
+  }
+  {
+    auto merge_case = [&](const char *name, const std::vector<int> &a, const std::vector<int> &b) {
+      std::vector<int> out(a.size() + b.size(), -1), ref(a.size() + b.size());
+      auto ret = std::merge(pol, a.begin(), a.end(), b.begin(), b.end(), out.begin());
+      auto hret = std::merge(a.begin(), a.end(), b.begin(), b.end(), ref.begin());
+      CHECK(out == ref, "stdpar merge %s", name);
+      CHECK(ret - out.begin() == hret - ref.begin(), "stdpar merge %s return", name);
+    };
+    merge_case("empty", {}, {});
+    merge_case("single 1 0", {2}, {});
+    merge_case("single 0 1", {}, {3});
+    merge_case("single 1 1", {2}, {3});
+    std::vector<int> lo(1024), hi(1024);
+    std::iota(lo.begin(), lo.end(), 0);
+    std::iota(hi.begin(), hi.end(), 1024);
+    merge_case("trivial", lo, hi);
+    merge_case("trivial swapped", hi, lo);
+    merge_case("same size", sorted_random(256, 123), sorted_random(256, 42));
+    merge_case("same data", sorted_random(1024, 123), sorted_random(1024, 123));
+    merge_case("v1 larger", sorted_random(1932, 123), sorted_random(1000, 42));
+    merge_case("v2 larger", sorted_random(1000, 123), sorted_random(1932, 42));
+  }
+  alg::util::allocation_cache cache{alg::util::allocation_type::device};
+  std::mt19937 gen(7);
+  auto by_key = [] __host__ __device__(const keyed &x, const keyed &y) { return x.key < y.key; };
+  for (size_t n : {2ul, 2047ul, 2048ul, 2049ul, 3 * 4096ul + 5, 1ul << 20}) {
+    std::vector<keyed> h(n);
+    std::uniform_int_distribution<int> dk(0, (int)std::max<size_t>(n / 16, 1));
+    for (size_t i = 0; i < n; ++i) h[i] = {dk(gen), (int)i};
+    keyed *d = to_dev(q, h);
+    alg::sort(q, d, d + n, by_key).wait();
+    std::stable_sort(h.begin(), h.end(), [](const keyed &x, const keyed &y) { return x.key < y.key; });
+    CHECK(from_dev(q, d, n) == h, "algorithms::sort stable with a lambda comparator n=%zu", n);
+    // merge two sorted halves (ties across the halves: a's first)
+    const size_t n1 = n / 3;
+    std::vector<keyed> a(h.begin(), h.begin() + n1), b(h.begin() + n1, h.end());
+    for (auto &x : b) x.idx += 1 << 30;
+    std::vector<keyed> ref(n);
+    std::merge(a.begin(), a.end(), b.begin(), b.end(), ref.begin(),
+               [](const keyed &x, const keyed &y) { return x.key < y.key; });
+    keyed *da = to_dev(q, a), *db = to_dev(q, b), *dout = sycl::malloc_device<keyed>(n, q);
+    {
+      alg::util::allocation_group g{&cache, q.get_device()};
+      alg::merge(q, g, da, da + n1, db, db + (n - n1), dout, by_key).wait();
+    }
+    CHECK(from_dev(q, dout, n) == ref, "algorithms::merge stable with a lambda comparator n=%zu", n);
+    sycl::free(dout, q);
+    sycl::free(db, q);
+    sycl::free(da, q);
+    sycl::free(d, q);
+  }
+  {
+    const size_t n = 1ul << 24;
+    std::vector<double> h(n);
+    std::normal_distribution<double> nd;
+    for (auto &v : h) v = nd(gen);
+    double *d = to_dev(q, h);
+    alg::sort(q, d, d + n, std::greater<>{}).wait();
+    std::sort(h.begin(), h.end(), std::greater<>{});
+    CHECK(from_dev(q, d, n) == h, "algorithms::sort f64 std::greater 2^24");
+    sycl::free(d, q);
+  }
+  {
+    const size_t n = 1ul << 24;
+    std::vector<uint32_t> h(n);
+    for (auto &v : h) v = (uint32_t)gen();
+    uint32_t *d = to_dev(q, h), *w = to_dev(q, h);
+    std::vector<uint32_t> ref = h;
+    std::sort(ref.begin(), ref.end());
+    alg::sort(q, d, d + n).wait();
+    CHECK(from_dev(q, d, n) == ref, "algorithms::sort u32 2^24");
+    // each run restores the random keys (a 64 MiB device copy) and sorts them
+    const float t = median_ms(q, [&] {
+      cudaMemcpyAsync(d, w, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, q.cuda_stream());
+      alg::sort(q, d, d + n);
+    }, 5);
+    std::printf("TIMING u32 2^24 random sort (+ key restore copy): %.4f ms\n", t);
+    CHECK(from_dev(q, d, n) == ref, "algorithms::sort u32 2^24 after timing");
+    sycl::free(w, q);
+    sycl::free(d, q);
+  }
+}
+
+// ----------------------------------------------- workload configurations
+// Config 1: 2^24 int32 U[-1000, 1000] (seed 0) through the entry points it
+// names -- sycl::reduction in parallel_for, std::reduce and
+// std::inclusive_scan on the stdpar policy -- bit-exact against a host sum /
+// scan.  Config 3: hipsycl::algorithms::copy_if with a lambda predicate
+// (x & 7) < 3 on 2^28 uint32 (seed 4), bit-exact and order-preserving.
+// Config 2's fp32 values (seed 1) through sycl::reduction: within 1e-6 of a
+// float64 host sum.
 
 static void test_workload_configs(sycl::queue &q) {
   alg::util::allocation_cache cache{alg::util::allocation_type::device};
@@ -704,6 +824,7 @@ int main() {
     test_group_functions(q);
     test_atomics(q);
     test_stdpar();
+    test_sort_merge(q);
     test_workload_configs(q);
   } catch (const std::exception &e) {
     std::printf("FAIL exception: %s\n", e.what());

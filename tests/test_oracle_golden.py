@@ -167,3 +167,24 @@ def test_single_write_scan_tiles_and_threads():
         assert np.array_equal(i, runs[0][1])
     ref = (7 + np.concatenate([[0], np.cumsum(xi.astype(np.int64))[:-1]])).astype(np.int32)
     assert np.array_equal(runs[0][1], ref)
+
+
+def test_oracle_merge_sort_against_reference_test_cases():
+    """The oracle's stable merge / sort reproduce the known answers of the
+    reference's tests/pstl/merge.cpp and sort.cpp (std::merge / std::sort
+    outputs generated by tests/golden/make_merge_sort.py), and keep the
+    stable order of equal keys with different bits in both directions."""
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "merge_sort_cases.npz"))
+    names = sorted({k.rsplit("/", 1)[0] for k in g.files})
+    assert len(names) == 16
+    for nm in names:
+        if nm.startswith("merge/"):
+            assert np.array_equal(O.merge(g[nm + "/a"], g[nm + "/b"]), g[nm + "/out"]), nm
+        else:
+            assert np.array_equal(O.sort(g[nm + "/in"]), g[nm + "/out"]), nm
+    x = np.array([1.0, -0.0, 0.0, 1.0, -0.0, 2.0], dtype=np.float32)
+    assert np.signbit(O.sort(x)).tolist() == [True, False, True, False, False, False]
+    assert np.signbit(O.sort(x, True)).tolist() == [False, False, False, True, False, True]
+    a = np.array([0.0, 1.0], dtype=np.float64)
+    b = np.array([-0.0, 1.0], dtype=np.float64)
+    assert np.signbit(O.merge(a, b)).tolist() == [False, True, False, False]
