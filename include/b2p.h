@@ -89,7 +89,8 @@ typedef enum b2p_prim {
   B2P_PRIM_DOT = 4,
   B2P_PRIM_SEG_REDUCE = 5,
   B2P_PRIM_SEG_SCAN = 6,
-  B2P_PRIM_SORT = 7 /* scratch sizing only */
+  B2P_PRIM_SORT = 7,  /* scratch sizing only */
+  B2P_PRIM_MERGE = 8  /* scratch sizing only (n = total keys) */
 } b2p_prim;
 
 /* copy_if predicate family: (x & mask) CMP rhs on the element's bits */
@@ -259,16 +260,21 @@ int b2p_segmented_per_call(int prim, int dtype, int op, const void *in, void *ou
  * out[0..na+nb) (ascending, or descending when descending != 0; on equal
  * keys the elements of a come first).  dtype I32, I64, U32, U64, F32, F64;
  * floats compare with < (NaNs unordered).  One pass: merge-path tiles.
+ * scratch: device memory of at least b2p_scratch_bytes(B2P_PRIM_MERGE,
+ * dtype, na + nb, 0, B2P_CONFIG_AUTO) bytes (the tile starts; no
+ * initialisation needed, and like b2p_sort's not a look-back scratch
+ * buffer of the other primitives).
  * Replaces hipsycl::algorithms::merge (algorithms/algorithm.hpp:519-560,
  * algorithms/merge/merge.hpp:222-313) for these types with std::less /
  * std::greater. */
 int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
-              b2p_stream stream);
+              void *scratch, size_t scratch_bytes, b2p_stream stream);
 
 /* Sort keys[0..n) in place, ascending (descending != 0: descending),
  * stable.  dtype as b2p_merge.  scratch: device memory of at least
  * b2p_scratch_bytes(B2P_PRIM_SORT, dtype, n, 0, B2P_CONFIG_AUTO) bytes (a
- * second array of n keys; its contents need no initialisation).  The sort
+ * second array of n keys and the merge passes' tile starts; its contents
+ * need no initialisation).  The sort
  * overwrites it with keys, so it must not be a scratch buffer that the
  * other primitives use for their look-back status words.  A merge
  * sort: tiles sorted in shared memory, then log2(n / tile) merge passes.

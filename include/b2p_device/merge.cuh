@@ -6,12 +6,13 @@
 // merge-path partitioning, hierarchical hybrid merge) and sort
 // (algorithms/sort/bitonic_sort.hpp:69-110: an in-place bitonic network of
 // log2(n)^2 / 2 global passes) with:
-//   merge  one pass over the output in tiles: each block finds its tile's
-//          split of the two inputs on the merge path (binary search along
-//          the tile's first diagonal), stages both input ranges in shared
-//          memory, and every thread merges its ITEMS outputs after its own
-//          merge-path search in shared memory; outputs leave in coalesced
-//          rows.  Reads each input once, writes each output once.
+//   merge  one pass over the output in tiles: a partition kernel finds
+//          where every tile starts on the merge path (one warp per tile,
+//          a 32-way search along the tile's first diagonal), then each
+//          block stages its tile's two input ranges in shared memory and
+//          every thread merges its ITEMS outputs after its own merge-path
+//          search in shared memory; outputs leave in coalesced rows.
+//          Reads each input once, writes each output once.
 //   sort   a merge sort: blocks sort tiles in shared memory (a stable
 //          odd-even sort of each thread's ITEMS keys in registers, then
 //          log2(threads) rounds of merge-path merges of runs in shared
@@ -107,44 +108,67 @@ __device__ __forceinline__ void merge_serial(const T *a, int ia, int na, const T
   }
 }
 
+// Where each tile starts on its merge path, for the pairwise merge of runs
+// of length `run` (PAIRS; a == b == src, na = n, nb = 0) or the one merge
+// of a[0..na) and b[0..nb): one warp per tile, splits[t] = the number of
+// keys of the tile's first range (A) before the tile's first output.  All
+// searches run at once, so the merge kernel starts loading at once.
+template <class T>
+struct PairView {
+  const T *A, *B;
+  long long nA, nB, base;
+};
+
+template <class T, bool PAIRS>
+__device__ __forceinline__ PairView<T> pair_of(const T *a, long long na, const T *b, long long nb, long long run,
+                                               long long d0) {
+  PairView<T> v{a, b, na, nb, 0};
+  if constexpr (PAIRS) {
+    v.base = d0 / (2 * run) * (2 * run);
+    v.A = a + v.base;
+    v.nA = min(run, na - v.base);
+    v.B = a + v.base + v.nA;
+    v.nB = min(run, na - v.base - v.nA);
+  }
+  return v;
+}
+
+template <class T, class Comp, bool PAIRS>
+__global__ void __launch_bounds__(256) merge_partition_kernel(const T *a, long long na, const T *b, long long nb,
+                                                              long long run, long long ntiles, long long *splits,
+                                                              Comp comp) {
+  constexpr int kMergeTile = merge_tile<T>();
+  const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= ntiles) return;  // whole warps leave together
+  const PairView<T> v = pair_of<T, PAIRS>(a, na, b, nb, run, t * kMergeTile);
+  const T *A = v.A, *B = v.B;
+  auto ga = [&](long long i) { return A[i]; };
+  auto gb = [&](long long i) { return B[i]; };
+  const long long sp = merge_path_warp<T>(ga, v.nA, gb, v.nB, t * kMergeTile - v.base, comp);
+  if ((threadIdx.x & 31) == 0) splits[t] = sp;
+}
+
 // Merge tile `blockIdx.x` of the pairwise merge of runs of length `run`
-// (run >= total: one pair, the merge of a[0..na) and b[0..nb) as given).
-// For the sort passes a == b == src with na = nb = n: the pair of output
-// position d is runs [2r, 2r + run) and [2r + run, 2r + 2 run), r = d / (2
-// run) * run.
+// (PAIRS) or of the one merge of a and b, from the tile starts in `splits`
+// (merge_partition_kernel).  The tile ends where the next tile starts, or,
+// for the last tile of its pair, at the end of both ranges.
 template <class T, class Comp, bool PAIRS>
 __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long long na, const T *b, long long nb,
-                                                              T *out, long long run, Comp comp) {
+                                                              T *out, long long run, const long long *splits,
+                                                              Comp comp) {
   constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
   __shared__ T s_in[kMergeTile];
   __shared__ T s_out[kMergeTile];
-  __shared__ long long s_split[2];
   const long long total = PAIRS ? na : na + nb;
   const long long d0 = (long long)blockIdx.x * kMergeTile;
   if (d0 >= total) return;
-  // the pair this tile belongs to (PAIRS), as two ranges A, B
-  const T *A = a;
-  const T *B = b;
-  long long nA = na, nB = nb, base = 0;
-  if constexpr (PAIRS) {
-    base = d0 / (2 * run) * (2 * run);
-    A = a + base;
-    nA = min(run, total - base);
-    B = a + base + nA;
-    nB = min(run, total - base - nA);
-  }
+  const PairView<T> v = pair_of<T, PAIRS>(a, na, b, nb, run, d0);
+  const T *A = v.A, *B = v.B;
   const long long tile_end = min(d0 + kMergeTile, total);
-  const long long l0 = d0 - base, l1 = tile_end - base;  // diagonals within the pair
-  auto ga = [&](long long i) { return A[i]; };
-  auto gb = [&](long long i) { return B[i]; };
-  // warp 0 finds where the tile starts on the merge path, warp 1 where it ends
-  if (threadIdx.x < 64) {
-    const long long sp = merge_path_warp<T>(ga, nA, gb, nB, threadIdx.x < 32 ? l0 : l1, comp);
-    if ((threadIdx.x & 31) == 0) s_split[threadIdx.x >> 5] = sp;
-  }
-  __syncthreads();
-  const long long i0 = s_split[0], i1 = s_split[1];
-  const long long j0 = l0 - i0, j1 = l1 - i1;
+  const long long l1 = tile_end - v.base;
+  const long long i0 = splits[blockIdx.x];
+  const long long i1 = l1 == v.nA + v.nB ? v.nA : splits[blockIdx.x + 1];
+  const long long j0 = (d0 - v.base) - i0, j1 = l1 - i1;
   const int na_t = (int)(i1 - i0), nb_t = (int)(j1 - j0);
   for (int k = threadIdx.x; k < na_t + nb_t; k += kMergeThreads)
     s_in[k] = k < na_t ? A[i0 + k] : B[j0 + (k - na_t)];
@@ -154,11 +178,11 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long l
   auto sa = [&](long long i) { return s_in[i]; };
   auto sb = [&](long long i) { return s_in[na_t + i]; };
   const int it = (int)merge_path<T>(sa, na_t, sb, nb_t, dt, comp);
-  T v[kMergeItems];
-  merge_serial(s_in, it, na_t, s_in + na_t, dt - it, nb_t, v, min(kMergeItems, cnt - dt), comp);
+  T v_[kMergeItems];
+  merge_serial(s_in, it, na_t, s_in + na_t, dt - it, nb_t, v_, min(kMergeItems, cnt - dt), comp);
 #pragma unroll
   for (int k = 0; k < kMergeItems; ++k)
-    if (dt + k < cnt) s_out[dt + k] = v[k];
+    if (dt + k < cnt) s_out[dt + k] = v_[k];
   __syncthreads();
   for (int k = threadIdx.x; k < cnt; k += kMergeThreads) out[d0 + k] = s_out[k];
 }
@@ -224,38 +248,59 @@ __global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long
 
 // ------------------------------------------------------------------ host
 
-// Stable merge of a[0..na) and b[0..nb) into out (asynchronous on st).
+// Scratch of a merge of `total` keys: the tile starts.
+template <class T>
+inline size_t merge_scratch_bytes(size_t total) {
+  return ((total + merge_tile<T>() - 1) / merge_tile<T>() + 1) * sizeof(long long) + 256;
+}
+
+// Stable merge of a[0..na) and b[0..nb) into out (asynchronous on st);
+// scratch: merge_scratch_bytes<T>(na + nb) bytes of device memory.
 template <class T, class Comp>
-int launch_merge(const T *a, size_t na, const T *b, size_t nb, T *out, const Comp &comp, cudaStream_t st) {
+int launch_merge(const T *a, size_t na, const T *b, size_t nb, T *out, const Comp &comp, void *scratch,
+                 size_t scratch_bytes, cudaStream_t st) {
   const long long total = (long long)(na + nb);
   if (total == 0) return B2P_OK;
   const long long tiles = (total + merge_tile<T>() - 1) / merge_tile<T>();
-  if (tiles > 0x7fffffffLL) return B2P_ERR_INVALID_ARG;
+  if (tiles > 0x7fffffffLL / 32) return B2P_ERR_INVALID_ARG;
+  if (!scratch || scratch_bytes < merge_scratch_bytes<T>((size_t)total) - 256) return B2P_ERR_SCRATCH;
+  long long *splits = reinterpret_cast<long long *>(scratch);
+  merge_partition_kernel<T, Comp, false><<<(unsigned)((tiles * 32 + 255) / 256), 256, 0, st>>>(
+      a, (long long)na, b, (long long)nb, total, tiles, splits, comp);
   merge_kernel<T, Comp, false><<<(unsigned)tiles, kMergeThreads, 0, st>>>(a, (long long)na, b, (long long)nb, out,
-                                                                          total, comp);
+                                                                          total, splits, comp);
   return cudaGetLastError() == cudaSuccess ? B2P_OK : B2P_ERR_CUDA;
 }
 
-// Scratch a sort of n keys of T needs (a second array of n keys).
+// Scratch a sort of n keys of T needs: a second array of n keys, then the
+// tile starts of the merge passes.
+template <class T>
+inline size_t sort_keys_bytes(size_t n) {
+  return (n * sizeof(T) + 255) / 256 * 256;
+}
 template <class T>
 inline size_t sort_scratch_bytes(size_t n) {
-  return n * sizeof(T) + 256;
+  return sort_keys_bytes<T>(n) + merge_scratch_bytes<T>(n);
 }
 
-// Stable merge sort of keys[0..n) in place; scratch holds n keys of T.
+// Stable merge sort of keys[0..n) in place; scratch: sort_scratch_bytes<T>(n)
+// bytes of device memory (none when n fits one tile).
 template <class T, class Comp>
 int launch_sort(T *keys, size_t n, const Comp &comp, void *scratch, size_t scratch_bytes, cudaStream_t st) {
   if (n <= 1) return B2P_OK;
   constexpr long long kMergeTile = merge_tile<T>();
   const long long tiles = ((long long)n + kMergeTile - 1) / kMergeTile;
-  if (tiles > 0x7fffffffLL) return B2P_ERR_INVALID_ARG;
+  if (tiles > 0x7fffffffLL / 32) return B2P_ERR_INVALID_ARG;
+  if (tiles > 1 && (!scratch || scratch_bytes < sort_scratch_bytes<T>(n) - 256)) return B2P_ERR_SCRATCH;
   block_sort_kernel<T, Comp><<<(unsigned)tiles, kMergeThreads, 0, st>>>(keys, (long long)n, comp);
   if (tiles == 1) return cudaGetLastError() == cudaSuccess ? B2P_OK : B2P_ERR_CUDA;
-  if (!scratch || scratch_bytes < n * sizeof(T)) return B2P_ERR_SCRATCH;
   T *src = keys, *dst = reinterpret_cast<T *>(scratch);
+  long long *splits = reinterpret_cast<long long *>(reinterpret_cast<char *>(scratch) + sort_keys_bytes<T>(n));
   for (long long run = kMergeTile; run < (long long)n; run *= 2) {
+    merge_partition_kernel<T, Comp, true><<<(unsigned)((tiles * 32 + 255) / 256), 256, 0, st>>>(
+        src, (long long)n, src, 0, run, tiles, splits, comp);
     merge_kernel<T, Comp, true><<<(unsigned)tiles, kMergeThreads, 0, st>>>(src, (long long)n, src, 0, dst, run,
-                                                                          comp);
+                                                                          splits, comp);
     T *x = src;
     src = dst;
     dst = x;

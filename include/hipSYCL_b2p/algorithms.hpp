@@ -893,8 +893,8 @@ b2p_sycl::event none_of(b2p_sycl::queue &q, ForwardIt first, ForwardIt last, det
 // compiled into the caller; non-pointer iterators are gathered into a
 // contiguous buffer first and scattered back after.  The reference's sort is
 // an in-place bitonic network without scratch; this one needs a second
-// array of n keys, taken from the stream-ordered allocator of the queue's
-// stream and released in stream order.
+// array of n keys (and the merge passes' tile starts): the queue's working
+// buffer, kept across calls.
 
 namespace detail {
 
@@ -954,16 +954,14 @@ b2p_sycl::event sort(b2p_sycl::queue &q, RandomIt first, RandomIt last, Compare 
     detail::gather_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(first, n, keys);
   }
   void *tmp = nullptr;
-  const size_t tmp_bytes = n * sizeof(T) + 256;
-  if (n > (size_t)::b2p::merge_tile<T>())
-    b2p_sycl::detail::check_cuda(cudaMallocAsync(&tmp, tmp_bytes, st), "sort: scratch");
+  const size_t tmp_bytes = ::b2p::sort_scratch_bytes<T>(n);
+  if (n > (size_t)::b2p::merge_tile<T>()) tmp = q.work_buffer(tmp_bytes);
   int rc;
   constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
   if constexpr (dt >= 0 && ord != 0)
     rc = b2p_sort(dt, keys, n, ord == 2, tmp, tmp ? tmp_bytes : 0, (b2p_stream)st);
   else
     rc = ::b2p::launch_sort(keys, n, comp, tmp, tmp ? tmp_bytes : 0, st);
-  if (tmp) cudaFreeAsync(tmp, st);
   if constexpr (!contiguous) {
     detail::scatter_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(keys, n, first);
     cudaFreeAsync(keys, st);
@@ -1006,12 +1004,14 @@ b2p_sycl::event merge(b2p_sycl::queue &q, util::allocation_group &scratch, Forwa
   T *out = nullptr;
   if constexpr (direct_out) out = &*d_first;
   else out = scratch.obtain<T>(n1 + n2);
+  const size_t sb = ::b2p::merge_scratch_bytes<T>(n1 + n2);
+  void *splits = scratch.obtain<unsigned char>(sb);
   int rc;
   constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
   if constexpr (dt >= 0 && ord != 0)
-    rc = b2p_merge(dt, a, n1, b, n2, out, ord == 2, (b2p_stream)st);
+    rc = b2p_merge(dt, a, n1, b, n2, out, ord == 2, splits, sb, (b2p_stream)st);
   else
-    rc = ::b2p::launch_merge(a, n1, b, n2, out, comp, st);
+    rc = ::b2p::launch_merge(a, n1, b, n2, out, comp, splits, sb, st);
   b2p_sycl::detail::check_b2p(rc, "merge");
   if constexpr (!direct_out)
     detail::scatter_kernel<T><<<detail::copy_grid(n1 + n2), detail::kGB, 0, st>>>(out, n1 + n2, d_first);

@@ -977,11 +977,12 @@ struct reduction_source : ::b2p::ValueSource<reduction_source<T, Op, K>, T> {
 
 // Scratch of one queue for the library's kernels: grown on demand (the
 // queue waits for its own work before a larger buffer replaces the old one),
-// zero-filled on allocation, freed with the queue.  Calls on one queue run
-// in stream order, so they can share it.
+// zero-filled on allocation when `zero_fill` (the look-back scratch, whose
+// status words must start at zero), freed with the queue.  Calls on one
+// queue run in stream order, so they can share it.
 class queue_scratch {
  public:
-  explicit queue_scratch(int dev) : dev_(dev) {}
+  explicit queue_scratch(int dev, bool zero_fill = true) : dev_(dev), zero_fill_(zero_fill) {}
   queue_scratch(const queue_scratch &) = delete;
   queue_scratch &operator=(const queue_scratch &) = delete;
   ~queue_scratch() {
@@ -1002,7 +1003,7 @@ class queue_scratch {
       }
       const size_t b = std::max<size_t>(bytes, 64 * 1024);
       check_cuda(cudaMalloc(&p_, b), "queue scratch");
-      check_cuda(cudaMemsetAsync(p_, 0, b, s), "queue scratch");
+      if (zero_fill_) check_cuda(cudaMemsetAsync(p_, 0, b, s), "queue scratch");
       bytes_ = b;
     }
     return p_;
@@ -1011,6 +1012,7 @@ class queue_scratch {
 
  private:
   int dev_;
+  bool zero_fill_;
   std::mutex mu_;
   void *p_ = nullptr;
   size_t bytes_ = 0;
@@ -1031,7 +1033,13 @@ class queue {
     detail::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = std::shared_ptr<CUstream_st>(s, [](cudaStream_t p) { cudaStreamDestroy(p); });
     scratch_ = std::make_shared<detail::queue_scratch>(dev_.cuda_ordinal());
+    work_ = std::make_shared<detail::queue_scratch>(dev_.cuda_ordinal(), false);
   }
+  // Working memory of the queue's library calls that overwrite it with data
+  // (the second key array of hipsycl::algorithms::sort): at least `bytes`,
+  // kept and reused by later calls in stream order.
+  void *work_buffer(size_t bytes) { return work_->get(bytes, cuda_stream()); }
+  size_t work_buffer_size() const { return work_->size(); }
   device get_device() const { return dev_; }
   cudaStream_t cuda_stream() const { return stream_.get(); }
   bool is_in_order() const { return true; }
@@ -1144,6 +1152,7 @@ class queue {
   device dev_;
   std::shared_ptr<CUstream_st> stream_;
   std::shared_ptr<detail::queue_scratch> scratch_;
+  std::shared_ptr<detail::queue_scratch> work_;
 };
 
 // handler: the command-group form q.submit([&](handler& h) { ... }).

@@ -29,7 +29,7 @@ OK, ERR_INVALID_ARG, ERR_INVALID_PTR, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ER
 I32, I64, U32, U64, F32, BF16, F64 = range(7)
 SUM, PROD, MIN, MAX, AND, OR, XOR = range(7)
 PRIM_REDUCE, PRIM_SCAN, PRIM_COPY_IF, PRIM_HISTOGRAM, PRIM_DOT, PRIM_SEG_REDUCE, PRIM_SEG_SCAN, \
-    PRIM_SORT = range(8)
+    PRIM_SORT, PRIM_MERGE = range(9)
 CMP_LT, CMP_LE, CMP_EQ, CMP_NE, CMP_GE, CMP_GT = range(6)
 NUM_CONFIGS = 48
 AUTO = -1
@@ -84,7 +84,7 @@ def _declare(L):
         "b2p_scan": ([i, i, i, vp, vp, sz, vp, vp, sz, i, vp], i),
         "b2p_copy_if": ([i, vp, vp, sz, u64, i, u64, vp, vp, sz, i, vp], i),
         "b2p_histogram_u8": ([vp, sz, vp, i, i, vp], i),
-        "b2p_merge": ([i, vp, sz, vp, sz, vp, i, vp], i),
+        "b2p_merge": ([i, vp, sz, vp, sz, vp, i, vp, sz, vp], i),
         "b2p_sort": ([i, vp, sz, i, vp, sz, vp], i),
         "b2p_segmented_reduce": ([i, i, vp, vp, i64, vp, vp, vp, sz, i, vp], i),
         "b2p_segmented_scan": ([i, i, i, vp, vp, vp, i64, vp, vp, sz, i, vp], i),
@@ -297,15 +297,22 @@ def histogram_u8(keys, bins=None, nbins=256, config: int = AUTO, stream=None):
 
 def merge(a, b, out=None, descending=False, stream=None):
     """Stable merge of two sorted 1-D tensors of one dtype (elements of `a`
-    first on equal keys), like std::merge with std::less / std::greater."""
+    first on equal keys), like std::merge with std::less / std::greater.
+    The tile starts go to a buffer of their own (not the per-stream
+    look-back scratch)."""
     torch = _torch()
     code = dtype_code(a)
     if dtype_code(b) != code:
         raise ValueError("merge: a and b must have the same dtype")
+    total = a.numel() + b.numel()
     if out is None:
-        out = torch.empty(a.numel() + b.numel(), dtype=a.dtype, device=a.device)
+        out = torch.empty(total, dtype=a.dtype, device=a.device)
+    nbytes = lib().b2p_scratch_bytes(PRIM_MERGE, code, total, 0, AUTO)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    with torch.cuda.stream(s):
+        tmp = torch.empty(nbytes, dtype=torch.uint8, device=a.device)
     check(lib().b2p_merge(code, a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
-                          int(bool(descending)), _stream(stream)), "b2p_merge")
+                          int(bool(descending)), tmp.data_ptr(), nbytes, _stream(stream)), "b2p_merge")
     return out
 
 

@@ -223,7 +223,8 @@ size_t b2p_scratch_bytes(int prim, int dtype, size_t n, int64_t nseg, int config
   case B2P_PRIM_SEG_SCAN:
     return segmented_scratch_bytes(dtype, n, nseg, config);
   case B2P_PRIM_SORT:
-    return n * dtype_size(dtype) + 256;
+  case B2P_PRIM_MERGE:
+    return merge_sort_scratch_bytes(prim, dtype, n);
   default:
     return 0;
   }

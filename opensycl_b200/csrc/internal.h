@@ -39,6 +39,10 @@ long long debug_stall_tile();
 // Record a CUDA failure; returns B2P_ERR_CUDA or B2P_OK.
 int cuda_status(cudaError_t e);
 
+// Scratch bytes of b2p_sort (prim B2P_PRIM_SORT) or b2p_merge
+// (B2P_PRIM_MERGE) on n keys of dtype; 0 for other dtypes.
+size_t merge_sort_scratch_bytes(int prim, int dtype, size_t n);
+
 // Device-accessibility and alignment check of a pointer (B2P_OK or
 // B2P_ERR_INVALID_PTR); no CPU fallback.
 int check_pointer(const void *p, size_t align);

@@ -18,10 +18,17 @@ struct Greater {
 };
 
 template <class T>
-int merge_t(const void *a, size_t na, const void *b, size_t nb, void *out, bool desc, cudaStream_t st) {
+int merge_t(const void *a, size_t na, const void *b, size_t nb, void *out, bool desc, void *scratch, size_t sb,
+            cudaStream_t st) {
   const T *pa = reinterpret_cast<const T *>(a), *pb = reinterpret_cast<const T *>(b);
   T *po = reinterpret_cast<T *>(out);
-  return desc ? launch_merge(pa, na, pb, nb, po, Greater<T>{}, st) : launch_merge(pa, na, pb, nb, po, Less<T>{}, st);
+  return desc ? launch_merge(pa, na, pb, nb, po, Greater<T>{}, scratch, sb, st)
+              : launch_merge(pa, na, pb, nb, po, Less<T>{}, scratch, sb, st);
+}
+
+template <class T>
+size_t scratch_t(int prim, size_t n) {
+  return prim == B2P_PRIM_SORT ? sort_scratch_bytes<T>(n) : merge_scratch_bytes<T>(n);
 }
 
 template <class T>
@@ -34,26 +41,44 @@ bool sortable(int dtype) { return dtype >= B2P_I32 && dtype <= B2P_F64 && dtype 
 
 }  // namespace
 
+size_t merge_sort_scratch_bytes(int prim, int dtype, size_t n) {
+  switch (dtype) {
+  case B2P_I32: return scratch_t<int32_t>(prim, n);
+  case B2P_I64: return scratch_t<long long>(prim, n);
+  case B2P_U32: return scratch_t<uint32_t>(prim, n);
+  case B2P_U64: return scratch_t<unsigned long long>(prim, n);
+  case B2P_F32: return scratch_t<float>(prim, n);
+  case B2P_F64: return scratch_t<double>(prim, n);
+  default: return 0;
+  }
+}
+
 }  // namespace b2p
 
 using namespace b2p;
 
 extern "C" int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
-                         b2p_stream stream) {
+                         void *scratch, size_t scratch_bytes, b2p_stream stream) {
   if (!sortable(dtype)) return dtype == B2P_BF16 ? B2P_ERR_UNSUPPORTED : B2P_ERR_INVALID_ARG;
   if (na + nb == 0) return B2P_OK;
   const size_t es = dtype_size(dtype);
   int rc;
   if ((na && (rc = check_pointer(a, es))) || (nb && (rc = check_pointer(b, es))) || (rc = check_pointer(out, es)))
     return rc;
+  if (!scratch || scratch_bytes + 256 < merge_sort_scratch_bytes(B2P_PRIM_MERGE, dtype, na + nb) ||
+      check_pointer(scratch, 8))
+    return B2P_ERR_SCRATCH;
   cudaStream_t st = (cudaStream_t)stream;
+  const bool d = descending != 0;
+  void *s = scratch;
+  const size_t sb = scratch_bytes;
   switch (dtype) {
-  case B2P_I32: return merge_t<int32_t>(a, na, b, nb, out, descending, st);
-  case B2P_I64: return merge_t<long long>(a, na, b, nb, out, descending, st);
-  case B2P_U32: return merge_t<uint32_t>(a, na, b, nb, out, descending, st);
-  case B2P_U64: return merge_t<unsigned long long>(a, na, b, nb, out, descending, st);
-  case B2P_F32: return merge_t<float>(a, na, b, nb, out, descending, st);
-  default: return merge_t<double>(a, na, b, nb, out, descending, st);
+  case B2P_I32: return merge_t<int32_t>(a, na, b, nb, out, d, s, sb, st);
+  case B2P_I64: return merge_t<long long>(a, na, b, nb, out, d, s, sb, st);
+  case B2P_U32: return merge_t<uint32_t>(a, na, b, nb, out, d, s, sb, st);
+  case B2P_U64: return merge_t<unsigned long long>(a, na, b, nb, out, d, s, sb, st);
+  case B2P_F32: return merge_t<float>(a, na, b, nb, out, d, s, sb, st);
+  default: return merge_t<double>(a, na, b, nb, out, d, s, sb, st);
   }
 }
 
@@ -65,8 +90,8 @@ extern "C" int b2p_sort(int dtype, void *keys, size_t n, int descending, void *s
   int rc = check_pointer(keys, es);
   if (rc) return rc;
   if (n > (size_t)merge_tile<long long>()) {
-    if (!scratch || scratch_bytes < n * es) return B2P_ERR_SCRATCH;
-    if ((rc = check_pointer(scratch, es))) return B2P_ERR_SCRATCH;
+    if (!scratch || scratch_bytes + 256 < merge_sort_scratch_bytes(B2P_PRIM_SORT, dtype, n)) return B2P_ERR_SCRATCH;
+    if ((rc = check_pointer(scratch, 256))) return B2P_ERR_SCRATCH;
   }
   cudaStream_t st = (cudaStream_t)stream;
   switch (dtype) {

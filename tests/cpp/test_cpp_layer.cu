@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <numeric>
+#include <functional>
 #include <random>
+#include <string>
 #include <vector>
 
 namespace alg = hipsycl::algorithms;
@@ -770,7 +772,10 @@ static void test_workload_configs(sycl::queue &q) {
         q.parallel_for(sycl::range<1>(n), sycl::reduction(sum, sycl::plus<float>{}),
                        [=] __device__(sycl::id<1> i, auto &r) { r += d[i[0]]; });
       });
-      const float t_lib = median_ms(q, [&] { alg::reduce(q, g, d, d + n, r2, 0.f, sycl::plus<float>{}); });
+      const float t_lib = median_ms(q, [&] {
+        alg::util::allocation_group g1{&cache, q.get_device()};
+        alg::reduce(q, g1, d, d + n, r2, 0.f, sycl::plus<float>{});
+      });
       std::printf("TIMING fp32 2^28 sum: sycl::reduction %.4f ms, b2p_reduce %.4f ms, ratio %.3f\n", t_red, t_lib,
                   t_red / t_lib);
       CHECK(t_red <= 1.25f * t_lib, "sycl::reduction 2^28 within 25%% of b2p_reduce (%.4f vs %.4f ms)", t_red, t_lib);
@@ -799,11 +804,18 @@ static void test_workload_configs(sycl::queue &q) {
     std::vector<uint32_t> got = from_dev(q, out, ref.size());
     CHECK(got == ref, "config 3 lambda copy_if values");
     {
-      alg::util::allocation_group g{&cache, q.get_device()};
+      // one allocation group per call, as a caller of the algorithms library
+      // has: its scratch returns to the cache and the next call reuses it
       auto lam = [] __host__ __device__(uint32_t v) { return (v & 7u) < 3u; };
       const alg::mask_compare<uint32_t> mc{7u, 3u, B2P_CMP_LT};
-      const float t_lam = median_ms(q, [&] { alg::copy_if(q, g, d, d + n, out, lam, cnt); });
-      const float t_lib = median_ms(q, [&] { alg::copy_if(q, g, d, d + n, out, mc, cnt); });
+      const float t_lam = median_ms(q, [&] {
+        alg::util::allocation_group g{&cache, q.get_device()};
+        alg::copy_if(q, g, d, d + n, out, lam, cnt);
+      });
+      const float t_lib = median_ms(q, [&] {
+        alg::util::allocation_group g{&cache, q.get_device()};
+        alg::copy_if(q, g, d, d + n, out, mc, cnt);
+      });
       std::printf("TIMING u32 2^28 copy_if: lambda %.4f ms, b2p_copy_if %.4f ms, ratio %.3f\n", t_lam, t_lib,
                   t_lam / t_lib);
       CHECK(t_lam <= 1.25f * t_lib, "lambda copy_if 2^28 within 25%% of b2p_copy_if (%.4f vs %.4f ms)", t_lam, t_lib);
@@ -816,16 +828,23 @@ static void test_workload_configs(sycl::queue &q) {
   }
 }
 
-int main() {
+// With arguments, only the named sections run (algorithms, reduction, group,
+// atomics, stdpar, sort_merge, workload), in the order given.
+int main(int argc, char **argv) {
   try {
     sycl::queue q;
-    test_algorithms(q);
-    test_reduction(q);
-    test_group_functions(q);
-    test_atomics(q);
-    test_stdpar();
-    test_sort_merge(q);
-    test_workload_configs(q);
+    const std::vector<std::pair<std::string, std::function<void()>>> sections = {
+        {"algorithms", [&] { test_algorithms(q); }},   {"reduction", [&] { test_reduction(q); }},
+        {"group", [&] { test_group_functions(q); }},   {"atomics", [&] { test_atomics(q); }},
+        {"stdpar", [&] { test_stdpar(); }},            {"sort_merge", [&] { test_sort_merge(q); }},
+        {"workload", [&] { test_workload_configs(q); }}};
+    if (argc < 2) {
+      for (auto &sec : sections) sec.second();
+    } else {
+      for (int i = 1; i < argc; ++i)
+        for (auto &sec : sections)
+          if (sec.first == argv[i]) sec.second();
+    }
   } catch (const std::exception &e) {
     std::printf("FAIL exception: %s\n", e.what());
     return 2;

@@ -134,6 +134,8 @@ def test_bf16_and_bad_args_are_rejected(dev):
     L = C.lib()
     a = dev_t(np.arange(8, dtype=np.int32))
     assert L.b2p_sort(C.I32, a.data_ptr(), 1 << 16, 0, None, 0, None) == C.ERR_SCRATCH
-    assert L.b2p_merge(99, a.data_ptr(), 8, a.data_ptr(), 8, a.data_ptr(), 0, None) == C.ERR_INVALID_ARG
+    o = torch.empty(16, dtype=torch.int32, device="cuda")
+    assert L.b2p_merge(99, a.data_ptr(), 8, a.data_ptr(), 8, o.data_ptr(), 0, None, 0, None) == C.ERR_INVALID_ARG
+    assert L.b2p_merge(C.I32, a.data_ptr(), 8, a.data_ptr(), 8, o.data_ptr(), 0, None, 0, None) == C.ERR_SCRATCH
     host = np.zeros(8, dtype=np.int32)
     assert L.b2p_sort(C.I32, host.ctypes.data, 8, 0, None, 0, None) == C.ERR_INVALID_PTR
