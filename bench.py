@@ -499,12 +499,16 @@ def _time_b2b(torch, fn, reps=10, warm=3):
     return e0.elapsed_time(e1) / reps
 
 
-def _time_op(torch, fn, reps=10, warm=3, flush=None):
+def _time_op(torch, fn, reps=10, warm=3, flush=None, pre=None):
     s = torch.cuda.current_stream()
     for _ in range(warm):
+        if pre is not None:
+            pre()
         fn()
     ts = []
     for _ in range(reps):
+        if pre is not None:
+            pre()  # untimed set-up of the launch's input
         if flush is not None:
             flush.sum()  # reads 512 MB: evicts L2 without leaving dirty lines to drain later
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -573,6 +577,37 @@ def measure_ops(C, torch, np, peak, log2n=28, reps=10):
     rec(f"copy_if_u32_{sz}", lambda: C.copy_if(xu, 7, C.CMP_LT, 3, out=yu, count=cnt),
         4 * n + 4 * kept, f"kept {kept} ({kept / n:.4f})")
     del xu, yu
+    # merge: two sorted halves of n int32 keys; sort: n random int32 keys,
+    # restored from a copy before each rep (outside the timed pair)
+    L = C.lib()
+    sh = C._stream(None)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    ma = torch.randint(-(1 << 31), 1 << 31, (n // 2,), generator=g, device="cuda", dtype=torch.int64)
+    ma = ma.to(torch.int32).sort().values
+    mb = torch.randint(-(1 << 31), 1 << 31, (n // 2,), generator=g, device="cuda", dtype=torch.int64)
+    mb = mb.to(torch.int32).sort().values
+    mo = torch.empty(n, dtype=torch.int32, device="cuda")
+    msb = L.b2p_scratch_bytes(C.PRIM_MERGE, C.I32, n, 0, C.AUTO)
+    mscr = torch.empty(msb, dtype=torch.uint8, device="cuda")
+    rec(f"merge_i32_{sz}", lambda: C.check(L.b2p_merge(C.I32, ma.data_ptr(), n // 2, mb.data_ptr(), n // 2,
+                                                       mo.data_ptr(), 0, mscr.data_ptr(), msb, sh)),
+        8 * n, "two sorted halves; partition + merge-path tiles")
+    del ma, mb
+    keys0 = torch.randint(-(1 << 31), 1 << 31, (n,), generator=g, device="cuda", dtype=torch.int64)
+    keys0 = keys0.to(torch.int32)
+    ssb = L.b2p_scratch_bytes(C.PRIM_SORT, C.I32, n, 0, C.AUTO)
+    sscr = torch.empty(ssb, dtype=torch.uint8, device="cuda")
+    tile = 4096
+    passes = max(0, (n - 1).bit_length() - (tile - 1).bit_length())
+    nbytes = 8 * n * (1 + passes) + (8 * n if passes % 2 else 0)
+    ms = _time_op(torch, lambda: C.check(L.b2p_sort(C.I32, mo.data_ptr(), n, 0, sscr.data_ptr(), ssb, sh)),
+                  reps=reps, flush=None, pre=lambda: mo.copy_(keys0))
+    gbs = nbytes / (ms / 1e3) / 1e9
+    ops[f"sort_i32_{sz}"] = {"ms": round(ms, 4), "Gkeys/s": round(n / ms / 1e6, 2), "GB/s": round(gbs, 1),
+                            "frac_hbm": round(gbs / peak, 4), "bytes": nbytes,
+                            "note": f"random keys; block sort of {tile}-key tiles + {passes} merge passes "
+                                    "(bytes = what those passes move)"}
+    del keys0, mo, mscr, sscr
     k = torch.from_numpy(C.synth_fill(4, 5, n, 1.2)).cuda()
     bins = torch.zeros(256, dtype=torch.int32, device="cuda")
     rec(f"histogram_u8_zipf1.2_{sz}", lambda: C.histogram_u8(k, bins=bins), n + 1024)

@@ -32,13 +32,14 @@
 namespace b2p {
 
 constexpr int kMergeThreads = 256;
-// Keys per thread: the two shared tiles of a block stay within 32 KiB.
+// Keys per thread: 64 bytes of keys (the block sort's two shared tiles stay
+// within 32 KiB), at most 16.
 template <class T>
-constexpr int merge_items() {
-  return sizeof(T) <= 8 ? 8 : (sizeof(T) <= 16 ? 4 : (sizeof(T) <= 32 ? 2 : 1));
+__host__ __device__ constexpr int merge_items() {
+  return sizeof(T) <= 4 ? 16 : (sizeof(T) <= 8 ? 8 : (sizeof(T) <= 16 ? 4 : (sizeof(T) <= 32 ? 2 : 1)));
 }
 template <class T>
-constexpr int merge_tile() {
+__host__ __device__ constexpr int merge_tile() {
   return kMergeThreads * merge_items<T>();
 }
 
@@ -91,21 +92,56 @@ __device__ __forceinline__ long long merge_path_warp(IdxA a, long long na, IdxB 
   return lo;
 }
 
-// Serial stable merge of `count` outputs starting at a[ia], b[ib] (shared
-// memory views), into out[0..count).
-template <class T, class Comp>
-__device__ __forceinline__ void merge_serial(const T *a, int ia, int na, const T *b, int ib, int nb, T *out,
-                                             int count, const Comp &comp) {
+// Shared-memory slot of tile element i: one pad slot after every 32, so
+// the threads of a warp, whose runs start ITEMS (a power of two) apart,
+// read and write 32 different banks.
+__device__ __forceinline__ int spad(int i) { return i + (i >> 5); }
+__host__ __device__ constexpr int spad_size(int n) { return n + n / 32; }
+
+// Serial stable merge of ITEMS outputs starting at a[ia], b[ib] of the two
+// ranges s[pad(a0 + i)] and s[pad(b0 + i)] of one padded shared array
+// into out[]; the current key of each range stays in a register, and each
+// output costs one shared load, without branches (the warp's threads take
+// different sides).  Outputs past the end of both ranges are left
+// unspecified.  Reads only slots a0 + [0, na), b0 + [0, nb) and slot 0,
+// which stands in for the next key of an exhausted side (its value is
+// never used).
+template <class T, int ITEMS, class Comp>
+__device__ __forceinline__ void merge_serial(const T *s, int a0, int ia, int na, int b0, int ib, int nb,
+                                             T (&out)[ITEMS], const Comp &comp) {
+  T va = s[spad(ia < na ? a0 + ia : 0)];
+  T vb = s[spad(ib < nb ? b0 + ib : 0)];
 #pragma unroll
-  for (int k = 0; k < merge_items<T>(); ++k) {
-    if (k < count) {
-      bool take_b;
-      if (ia >= na) take_b = true;
-      else if (ib >= nb) take_b = false;
-      else take_b = comp(b[ib], a[ia]);
-      out[k] = take_b ? b[ib++] : a[ia++];
+  for (int k = 0; k < ITEMS; ++k) {
+    const bool take_b = ib < nb && (ia >= na || comp(vb, va));
+    out[k] = take_b ? vb : va;
+    ia += take_b ? 0 : 1;
+    ib += take_b ? 1 : 0;
+    // the next key of the side just taken
+    const int nxt = take_b ? (ib < nb ? b0 + ib : 0) : (ia < na ? a0 + ia : 0);
+    const T v = s[spad(nxt)];
+    vb = take_b ? v : vb;
+    va = take_b ? va : v;
+  }
+}
+
+// Store the ITEMS keys of v to dst[0..count): 16-byte vector stores when the
+// whole run is there and dst is 16-byte aligned.
+template <class T, int ITEMS>
+__device__ __forceinline__ void store_run(T *dst, const T (&v)[ITEMS], int count) {
+  constexpr int kBytes = (int)sizeof(T) * ITEMS;
+  if constexpr (kBytes % 16 == 0) {
+    if (count == ITEMS && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+      uint4 w[kBytes / 16];
+      memcpy(w, v, kBytes);
+#pragma unroll
+      for (int j = 0; j < kBytes / 16; ++j) reinterpret_cast<uint4 *>(dst)[j] = w[j];
+      return;
     }
   }
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k)
+    if (k < count) dst[k] = v[k];
 }
 
 // Where each tile starts on its merge path, for the pairwise merge of runs
@@ -157,8 +193,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long l
                                                               T *out, long long run, const long long *splits,
                                                               Comp comp) {
   constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
-  __shared__ T s_in[kMergeTile];
-  __shared__ T s_out[kMergeTile];
+  __shared__ T s_in[spad_size(kMergeTile)];
   const long long total = PAIRS ? na : na + nb;
   const long long d0 = (long long)blockIdx.x * kMergeTile;
   if (d0 >= total) return;
@@ -170,32 +205,50 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long l
   const long long i1 = l1 == v.nA + v.nB ? v.nA : splits[blockIdx.x + 1];
   const long long j0 = (d0 - v.base) - i0, j1 = l1 - i1;
   const int na_t = (int)(i1 - i0), nb_t = (int)(j1 - j0);
-  for (int k = threadIdx.x; k < na_t + nb_t; k += kMergeThreads)
-    s_in[k] = k < na_t ? A[i0 + k] : B[j0 + (k - na_t)];
-  __syncthreads();
   const int cnt = na_t + nb_t;
+  if (cnt == kMergeTile) {
+    // a full tile: every thread's ITEMS loads in flight at once
+    const T *pa = A + i0, *pb = B + (j0 - na_t);
+    T r[kMergeItems];
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) {
+      const int k = threadIdx.x + q * kMergeThreads;
+      r[q] = (k < na_t ? pa : pb)[k];
+    }
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) s_in[spad(threadIdx.x + q * kMergeThreads)] = r[q];
+  } else {
+    for (int k = threadIdx.x; k < cnt; k += kMergeThreads)
+      s_in[spad(k)] = k < na_t ? A[i0 + k] : B[j0 + (k - na_t)];
+  }
+  __syncthreads();
   const int dt = min((int)threadIdx.x * kMergeItems, cnt);
-  auto sa = [&](long long i) { return s_in[i]; };
-  auto sb = [&](long long i) { return s_in[na_t + i]; };
+  auto sa = [&](long long i) { return s_in[spad((int)i)]; };
+  auto sb = [&](long long i) { return s_in[spad(na_t + (int)i)]; };
   const int it = (int)merge_path<T>(sa, na_t, sb, nb_t, dt, comp);
   T v_[kMergeItems];
-  merge_serial(s_in, it, na_t, s_in + na_t, dt - it, nb_t, v_, min(kMergeItems, cnt - dt), comp);
-#pragma unroll
-  for (int k = 0; k < kMergeItems; ++k)
-    if (dt + k < cnt) s_out[dt + k] = v_[k];
-  __syncthreads();
-  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) out[d0 + k] = s_out[k];
+  merge_serial(s_in, 0, it, na_t, na_t, dt - it, nb_t, v_, comp);
+  // each thread's outputs are contiguous: straight from registers
+  store_run(out + d0 + dt, v_, min(kMergeItems, cnt - dt));
 }
 
 // Sort tile `blockIdx.x` of keys[0..n) in place (stable).
 template <class T, class Comp>
 __global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long long n, Comp comp) {
   constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
-  __shared__ T s_a[kMergeTile];
-  __shared__ T s_b[kMergeTile];
+  __shared__ T s_a[spad_size(kMergeTile)];
+  __shared__ T s_b[spad_size(kMergeTile)];
   const long long t0 = (long long)blockIdx.x * kMergeTile;
   const int cnt = (int)min((long long)kMergeTile, n - t0);
-  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) s_a[k] = keys[t0 + k];
+  if (cnt == kMergeTile) {
+    T r[kMergeItems];
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) r[q] = keys[t0 + threadIdx.x + q * kMergeThreads];
+#pragma unroll
+    for (int q = 0; q < kMergeItems; ++q) s_a[spad(threadIdx.x + q * kMergeThreads)] = r[q];
+  } else {
+    for (int k = threadIdx.x; k < cnt; k += kMergeThreads) s_a[spad(k)] = keys[t0 + k];
+  }
   __syncthreads();
   // each thread: its ITEMS keys, sorted by odd-even transposition (stable:
   // neighbours swap only when the right one is strictly before the left)
@@ -204,7 +257,7 @@ __global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long
   T v[kMergeItems];
 #pragma unroll
   for (int k = 0; k < kMergeItems; ++k)
-    if (k < mine) v[k] = s_a[b0 + k];
+    if (k < mine) v[k] = s_a[spad(b0 + k)];
 #pragma unroll
   for (int r = 0; r < kMergeItems; ++r) {
 #pragma unroll
@@ -218,32 +271,38 @@ __global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long
   }
 #pragma unroll
   for (int k = 0; k < kMergeItems; ++k)
-    if (k < mine) s_a[b0 + k] = v[k];
+    if (k < mine) s_a[spad(b0 + k)] = v[k];
   __syncthreads();
   // rounds: runs of ITEMS, 2 ITEMS, ... merged pairwise in shared memory
   T *src = s_a, *dst = s_b;
   for (int run = kMergeItems; run < cnt; run *= 2) {
     const int d = b0;  // this thread's outputs [d, d + ITEMS)
+    const bool last = 2 * run >= cnt;  // the same for the whole block
     if (d < cnt) {
       const int pb = d / (2 * run) * (2 * run);
       const int la = min(run, cnt - pb), lb = max(0, min(run, cnt - pb - la));
-      const T *ra = src + pb, *rb = src + pb + la;
-      auto sa = [&](long long i) { return ra[i]; };
-      auto sb = [&](long long i) { return rb[i]; };
+      auto sa = [&](long long i) { return src[spad(pb + (int)i)]; };
+      auto sb = [&](long long i) { return src[spad(pb + la + (int)i)]; };
       const int dl = d - pb;
       const int ia = (int)merge_path<T>(sa, la, sb, lb, dl, comp);
       T w[kMergeItems];
-      merge_serial(ra, ia, la, rb, dl - ia, lb, w, min(kMergeItems, cnt - d), comp);
+      merge_serial(src, pb, ia, la, pb + la, dl - ia, lb, w, comp);
+      if (last) {  // the sorted tile leaves from registers
+        store_run(keys + t0 + d, w, min(kMergeItems, cnt - d));
+      } else {
 #pragma unroll
-      for (int k = 0; k < kMergeItems; ++k)
-        if (d + k < cnt) dst[d + k] = w[k];
+        for (int k = 0; k < kMergeItems; ++k)
+          if (d + k < cnt) dst[spad(d + k)] = w[k];
+      }
     }
+    if (last) return;
     __syncthreads();
     T *x = src;
     src = dst;
     dst = x;
   }
-  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) keys[t0 + k] = src[k];
+  // no merge round (cnt <= ITEMS): the first thread's sorted keys
+  for (int k = threadIdx.x; k < cnt; k += kMergeThreads) keys[t0 + k] = src[spad(k)];
 }
 
 // ------------------------------------------------------------------ host
