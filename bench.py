@@ -499,7 +499,14 @@ def _time_b2b(torch, fn, reps=10, warm=3):
     return e0.elapsed_time(e1) / reps
 
 
-def _time_op(torch, fn, reps=10, warm=3, flush=None, pre=None):
+def _time_op(torch, fn, reps=10, warm=3, flush=None, pre=None, hold_cycles=200000):
+    """Median device time of single launches of fn, one event pair around
+    each.  Before the start event the stream is kept busy on the GPU (the L2
+    flush, or a spin of `hold_cycles` clock cycles, about 0.1 ms), so the
+    host-side cost of enqueueing fn (Python, ctypes, argument checks) falls
+    inside that work instead of showing up as idle GPU time between the
+    events: the figure is the launch's own device time, ramp and drain
+    included."""
     s = torch.cuda.current_stream()
     for _ in range(warm):
         if pre is not None:
@@ -511,6 +518,8 @@ def _time_op(torch, fn, reps=10, warm=3, flush=None, pre=None):
             pre()  # untimed set-up of the launch's input
         if flush is not None:
             flush.sum()  # reads 512 MB: evicts L2 without leaving dirty lines to drain later
+        elif hold_cycles:
+            torch.cuda._sleep(hold_cycles)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         fn()

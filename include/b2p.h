@@ -31,6 +31,29 @@
  *    integer result; float results stay within the documented tolerance.
  *  - n == 0: outputs are left untouched and no kernel is launched, as in
  *    the reference (algorithms/numeric.hpp:165-169).
+ *  - Every call that launches work opens an NVTX range named after it
+ *    (b2p_reduce, b2p_scan, ...) for the duration of the host call.
+ *
+ * Environment (read once per process)
+ *  - B2P_LOG_LEVEL: see b2p_log_level().  Errors are logged at level >= 1,
+ *    one record per call (operation, dtype, n, segments, configuration,
+ *    status) at 3, and at 4 the call is timed on its stream and the record
+ *    adds milliseconds and GB/s.
+ *  - B2P_CHECKED=1: the extent of every pointer argument (elements x size)
+ *    must lie inside one device allocation, and segment offsets are copied
+ *    to the host and checked (non-decreasing, inside the input); a failed
+ *    check returns B2P_ERR_INVALID_PTR / B2P_ERR_INVALID_ARG before
+ *    anything is launched.  Off by default (the offsets check synchronises
+ *    the stream).
+ *  - B2P_SELECTOR: how B2P_CONFIG_AUTO chooses: "learned" (default: the
+ *    installed selector table, else the fixed heuristic), "heuristic", or
+ *    the path of a selector weights file (b2p_selector_save) that is loaded
+ *    and installed at the first AUTO call.
+ *  - B2P_SCAN_CHUNK_MB (default 16) and B2P_SCAN_LOOKAHEAD (default 2):
+ *    chunk size in MiB of input, and how many chunks the first phase runs
+ *    ahead of the second, of the two-phase scan kernel (persistent grid
+ *    modes 1 and 2 of the scan configurations that do not run the TMA
+ *    pipeline).  They change timing only, never results.
  */
 #ifndef B2P_H
 #define B2P_H
@@ -282,6 +305,14 @@ int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, voi
  * algorithms/sort/bitonic_sort.hpp:69-110). */
 int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
              b2p_stream stream);
+
+/* Log level of the library's stderr records (0 none, 1 errors, 2 warnings,
+ * 3 one line per call, 4 each call also timed on its stream, which makes
+ * the call wait for its work).  Initialised from B2P_LOG_LEVEL, else
+ * ACPP_DEBUG_LEVEL / HIPSYCL_DEBUG_LEVEL as the reference reads them
+ * (common/debug.hpp:14-21,61); default 2. */
+int b2p_log_level(void);
+void b2p_set_log_level(int level);
 
 /* Wait for `stream`, then read the sticky device error word kept in
  * `scratch` (B2P_OK or B2P_ERR_TIMEOUT); clear != 0 resets it.  scratch ==

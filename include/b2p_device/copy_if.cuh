@@ -64,6 +64,32 @@ __device__ __forceinline__ unsigned keep_bits(const uint32_t *w, const Pred &pre
   return keep;
 }
 
+// Exclusive scan of one 32-bit count per thread over the NC threads of a
+// warp group with one named barrier: warp totals through s_cnt (NC / 32
+// words, written again only after a later barrier of the group), then every
+// thread adds the totals of the warps before its own.
+template <int NC>
+__device__ __forceinline__ unsigned count_scan_1bar(unsigned v, unsigned *s_cnt, unsigned *total, int t, int bar) {
+  const int lane = t & 31, warp = t >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned o = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += o;
+  }
+  if (lane == 31) s_cnt[warp] = incl;
+  bar_named(bar, NC);
+  unsigned before = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < NC / 32; ++w) {
+    const unsigned c = s_cnt[w];
+    before += w < warp ? c : 0u;
+    tot += c;
+  }
+  *total = tot;
+  return before + incl - v;
+}
+
 template <class T, int NC, int ITEMS, class Pred>
 __global__ void __launch_bounds__(pipe_threads(NC), 1)
     copy_if_tmem_kernel(const __grid_constant__ CUtensorMap tin, TmaParams p, Pred pred) {
@@ -86,7 +112,7 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   unsigned *keep_all = reinterpret_cast<unsigned *>(smem + p.texcl_base);
   uint16_t *texcl_all = reinterpret_cast<uint16_t *>(keep_all + (size_t)p.slots * NC);  // offsets < 2^16
   __shared__ __align__(8) PipeState ps;
-  __shared__ unsigned long long s_warp[32];
+  __shared__ unsigned s_cnt[NC / 32];
   __shared__ int s_go[2];
 
   const int warp = threadIdx.x >> 5;
@@ -138,14 +164,16 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       }
       __syncwarp();
       if ((t & 31) == 0) mbar_arrive(&ps.empty[ri.s]);  // this warp is done with the input stage
+      // the predicate first: it waits for the shared loads, and the TMEM
+      // stores after it then issue without waiting
+      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
+      const unsigned keep = keep_bits<T, ITEMS>(w, pred, t * ITEMS, count);
       const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
       tmem_st16(ta, w);
       if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
-      const int count = (int)min((unsigned long long)kTile, p.n - (unsigned long long)tile * kTile);
-      const unsigned keep = keep_bits<T, ITEMS>(w, pred, t * ITEMS, count);
-      unsigned long long tile_kept;
-      const unsigned long long ex =
-          group_exclusive_scan<CountOps, NC>((unsigned long long)__popc(keep), s_warp, &tile_kept, t, 1);
+      unsigned kept32;
+      const unsigned ex = count_scan_1bar<NC>((unsigned)__popc(keep), s_cnt, &kept32, t, 1);
+      const unsigned long long tile_kept = kept32;
       texcl_all[(size_t)rs.s * NC + t] = (uint16_t)ex;
       keep_all[(size_t)rs.s * NC + t] = keep;
       tmem_wait_st();
@@ -183,7 +211,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       const long long tile = ps.tile[rs.s];
       const unsigned long long carry = ps.carry[rs.s];
       unsigned long long kept_total = ps.agg[rs.s];
-      if (carry > p.n || kept_total > p.n - carry) {  // only after a broken chain: write nothing
+      const bool broken = carry > p.n || kept_total > p.n - carry;
+      if (broken) {  // only after a broken chain: write nothing
         if (t == 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         kept_total = 0;
       }
@@ -199,31 +228,23 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       char *obuf = obase + (size_t)ro.s * p.out_stage_stride;
       const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
       const unsigned phase = (unsigned)(g0 & 15u);
-      const unsigned lim = (unsigned)kept_total;
+      if (!broken) {
+        T *ob = reinterpret_cast<T *>(obuf + phase) + o;  // phase is a multiple of sizeof(T)
+        unsigned pos = 0;
 #pragma unroll
-      for (int j = 0; j < ITEMS; ++j) {
-        const unsigned pos = o + __popc(keep & ((1u << j) - 1u));
-        if (((keep >> j) & 1u) && pos < lim) {
-          T v;
-          memcpy(&v, w + j * (int)(sizeof(T) / 4), sizeof(T));
-          *reinterpret_cast<T *>(obuf + phase + pos * sizeof(T)) = v;  // phase is a multiple of sizeof(T)
+        for (int j = 0; j < ITEMS; ++j) {
+          const unsigned b = (keep >> j) & 1u;
+          if (b) {
+            T v;
+            memcpy(&v, w + j * (int)(sizeof(T) / 4), sizeof(T));
+            ob[pos] = v;
+          }
+          pos += b;
         }
       }
       fence_async_smem();
-      bar_named(2, NC);
-      const uintptr_t g1 = g0 + kept_total * sizeof(T);
-      const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
-      const bool mid = a1 > a0;
-      const long long nhead = mid ? (long long)((a0 - g0) / sizeof(T)) : (long long)kept_total;
-      const long long tail0 = mid ? (long long)((a1 - g0) / sizeof(T)) : (long long)kept_total;
-      const long long ntl = (long long)kept_total - tail0;
-      if (t < nhead) out[carry + t] = *reinterpret_cast<const T *>(obuf + phase + t * sizeof(T));
-      if (t >= 32 && t - 32 < ntl) {
-        const long long k = tail0 + (t - 32);
-        out[carry + k] = *reinterpret_cast<const T *>(obuf + phase + k * sizeof(T));
-      }
+      bar_named(2, NC);  // the output stage is packed
       if (t == 0 && tile == last && p.num_copied) *p.num_copied = carry + kept_total;
-      bar_named(2, NC);  // the plain stores are done with the output stage
       if (t == 0) {
         ps.out_carry[ro.s] = carry;
         ps.out_count[ro.s] = kept_total;
@@ -249,8 +270,16 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         const uintptr_t g0 = reinterpret_cast<uintptr_t>(out + carry);
         const uintptr_t g1 = g0 + kept_total * sizeof(T);
         const uintptr_t a0 = (g0 + 15) & ~uintptr_t(15), a1 = g1 & ~uintptr_t(15);
+        const char *obuf = obase + (size_t)ro.s * p.out_stage_stride + (g0 & 15u);  // output element 0
+        // the elements before the first and after the last 16-byte boundary
+        // (fewer than 16 bytes each; all of them when no boundary pair
+        // encloses a block): plain stores
+        const long long nhead = a1 > a0 ? (long long)((a0 - g0) / sizeof(T)) : (long long)kept_total;
+        const long long tail0 = a1 > a0 ? (long long)((a1 - g0) / sizeof(T)) : (long long)kept_total;
+        for (long long k = 0; k < nhead; ++k) out[carry + k] = reinterpret_cast<const T *>(obuf)[k];
+        for (long long k = tail0; k < (long long)kept_total; ++k) out[carry + k] = reinterpret_cast<const T *>(obuf)[k];
         if (a1 > a0) {
-          const char *src = obase + (size_t)ro.s * p.out_stage_stride + (g0 & 15u) + (a0 - g0);
+          const char *src = obuf + (a0 - g0);
           asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(a0),
                        "r"(smem_u32(src)), "r"((unsigned)(a1 - a0))
                        : "memory");

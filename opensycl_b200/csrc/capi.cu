@@ -167,7 +167,8 @@ int validate_reduce(int dtype, int op, const void *in, size_t n, const void *out
 }
 
 static int resolve(int prim, int dtype, size_t n, int64_t nseg, int config) {
-  if (config == B2P_CONFIG_AUTO) return b2p_auto_config(prim, dtype, n, nseg, 0.0);
+  if (config == B2P_CONFIG_AUTO) config = b2p_auto_config(prim, dtype, n, nseg, 0.0);
+  note_config(config);
   return config;
 }
 
@@ -235,10 +236,11 @@ int b2p_scratch_init(void *scratch, size_t bytes, b2p_stream stream) {
   return cuda_status(cudaMemsetAsync(scratch, 0, bytes, (cudaStream_t)stream));
 }
 
-int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
+static int reduce_entry(int dtype, int op, const void *in, size_t n, void *out, const void *init,
                void *scratch, size_t scratch_bytes, int config, b2p_stream stream) {
   int rc = validate_reduce(dtype, op, in, n, out);
   if (rc || n == 0) return rc;
+  if ((rc = check_extent(in, n * dtype_size(dtype))) || (rc = check_extent(out, acc_size(dtype)))) return rc;
   if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_REDUCE, dtype, n, 0, config);
   if (!config_valid(B2P_PRIM_REDUCE, dtype, config)) return B2P_ERR_INVALID_ARG;
@@ -246,7 +248,13 @@ int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out, const voi
                        (cudaStream_t)stream);
 }
 
-int b2p_dot(int dtype, const void *a, const void *b, size_t n, void *out, const void *init,
+int b2p_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
+               void *scratch, size_t scratch_bytes, int config, b2p_stream stream) {
+  CallScope cs("b2p_reduce", dtype, n, 0, (double)n * dtype_size(dtype), stream);
+  return cs.done(reduce_entry(dtype, op, in, n, out, init, scratch, scratch_bytes, config, stream));
+}
+
+static int dot_entry(int dtype, const void *a, const void *b, size_t n, void *out, const void *init,
             void *scratch, size_t scratch_bytes, int config, b2p_stream stream) {
   if (dtype != B2P_F32 && dtype != B2P_BF16 && dtype != B2P_F64) return B2P_ERR_UNSUPPORTED;
   if (n == 0) return B2P_OK;
@@ -254,6 +262,9 @@ int b2p_dot(int dtype, const void *a, const void *b, size_t n, void *out, const 
   if (rc) return rc;
   if ((rc = check_ptr(a, dtype_size(dtype))) || (rc = check_ptr(b, dtype_size(dtype))) ||
       (rc = check_ptr(out, acc_size(dtype))))
+    return rc;
+  if ((rc = check_extent(a, n * dtype_size(dtype))) || (rc = check_extent(b, n * dtype_size(dtype))) ||
+      (rc = check_extent(out, acc_size(dtype))))
     return rc;
   if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_DOT, dtype, n, 0, config);
@@ -263,7 +274,13 @@ int b2p_dot(int dtype, const void *a, const void *b, size_t n, void *out, const 
                        (cudaStream_t)stream);
 }
 
-int b2p_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
+int b2p_dot(int dtype, const void *a, const void *b, size_t n, void *out, const void *init,
+            void *scratch, size_t scratch_bytes, int config, b2p_stream stream) {
+  CallScope cs("b2p_dot", dtype, n, 0, 2.0 * n * dtype_size(dtype), stream);
+  return cs.done(dot_entry(dtype, a, b, n, out, init, scratch, scratch_bytes, config, stream));
+}
+
+static int scan_entry(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
              const void *init, void *scratch, size_t scratch_bytes, int config,
              b2p_stream stream) {
   if (!valid_dtype(dtype) || !valid_op(dtype, op)) return B2P_ERR_INVALID_ARG;
@@ -272,6 +289,7 @@ int b2p_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t
   int rc = check_device();
   if (rc) return rc;
   if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, acc_size(dtype)))) return rc;
+  if ((rc = check_extent(in, n * dtype_size(dtype))) || (rc = check_extent(out, n * acc_size(dtype)))) return rc;
   if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_SCAN, dtype, n, 0, config);
   if (!config_valid(B2P_PRIM_SCAN, dtype, config)) return B2P_ERR_INVALID_ARG;
@@ -279,7 +297,14 @@ int b2p_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t
                      (cudaStream_t)stream);
 }
 
-int b2p_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
+int b2p_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t n,
+             const void *init, void *scratch, size_t scratch_bytes, int config,
+             b2p_stream stream) {
+  CallScope cs("b2p_scan", dtype, n, 0, (double)n * (dtype_size(dtype) + acc_size(dtype)), stream);
+  return cs.done(scan_entry(dtype, op, inclusive, in, out, n, init, scratch, scratch_bytes, config, stream));
+}
+
+static int copy_if_entry(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
                 uint64_t rhs, uint64_t *num_copied, void *scratch, size_t scratch_bytes,
                 int config, b2p_stream stream) {
   if (!valid_dtype(dtype) || dtype == B2P_BF16) return B2P_ERR_UNSUPPORTED;
@@ -293,6 +318,8 @@ int b2p_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, i
     return B2P_OK;
   }
   if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, dtype_size(dtype)))) return rc;
+  // the output must hold every element (all may be kept)
+  if ((rc = check_extent(in, n * dtype_size(dtype))) || (rc = check_extent(out, n * dtype_size(dtype)))) return rc;
   if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_COPY_IF, dtype, n, 0, config);
   if (!config_valid(B2P_PRIM_COPY_IF, dtype, config)) return B2P_ERR_INVALID_ARG;
@@ -300,21 +327,35 @@ int b2p_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, i
                         config, (cudaStream_t)stream);
 }
 
-int b2p_histogram_u8(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,
+int b2p_copy_if(int dtype, const void *in, void *out, size_t n, uint64_t mask, int cmp,
+                uint64_t rhs, uint64_t *num_copied, void *scratch, size_t scratch_bytes,
+                int config, b2p_stream stream) {
+  CallScope cs("b2p_copy_if", dtype, n, 0, (double)n * dtype_size(dtype), stream);
+  return cs.done(copy_if_entry(dtype, in, out, n, mask, cmp, rhs, num_copied, scratch, scratch_bytes, config, stream));
+}
+
+static int histogram_u8_entry(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,
                      b2p_stream stream) {
   if (nbins < 1 || nbins > 256) return B2P_ERR_INVALID_ARG;
   if (n == 0) return B2P_OK;
   int rc = check_device();
   if (rc) return rc;
   if ((rc = check_ptr(keys, 1)) || (rc = check_ptr(bins, 4))) return rc;
+  if ((rc = check_extent(keys, n)) || (rc = check_extent(bins, 4 * (size_t)nbins))) return rc;
   config = resolve(B2P_PRIM_HISTOGRAM, B2P_U32, n, 0, config);
   if (!config_valid(B2P_PRIM_HISTOGRAM, B2P_U32, config)) return B2P_ERR_INVALID_ARG;
   return launch_histogram_u8(keys, n, bins, nbins, config, (cudaStream_t)stream);
 }
 
-int b2p_segmented_reduce(int dtype, int op, const void *in, const int64_t *offsets, int64_t nseg,
-                         void *out, const void *init, void *scratch, size_t scratch_bytes,
-                         int config, b2p_stream stream) {
+int b2p_histogram_u8(const uint8_t *keys, size_t n, uint32_t *bins, int nbins, int config,
+                     b2p_stream stream) {
+  CallScope cs("b2p_histogram_u8", B2P_U32, n, 0, (double)n + 4.0 * nbins, stream);
+  return cs.done(histogram_u8_entry(keys, n, bins, nbins, config, stream));
+}
+
+static int segmented_reduce_entry(int dtype, int op, const void *in, const int64_t *offsets, int64_t nseg,
+                                  void *out, const void *init, void *scratch, size_t scratch_bytes, int config,
+                                  b2p_stream stream, CallScope &cs) {
   if (!valid_dtype(dtype) || !valid_op(dtype, op) || nseg < 0) return B2P_ERR_INVALID_ARG;
   if (nseg == 0) return B2P_OK;
   int rc = check_device();
@@ -322,7 +363,6 @@ int b2p_segmented_reduce(int dtype, int op, const void *in, const int64_t *offse
   if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, acc_size(dtype))) ||
       (rc = check_ptr(offsets, 8)))
     return rc;
-  if (!scratch) return B2P_ERR_SCRATCH;
   // total element count is needed on the host: read offsets[nseg]
   int64_t total = 0;
   cudaError_t e = cudaMemcpyAsync(&total, offsets + nseg, sizeof(int64_t), cudaMemcpyDefault,
@@ -330,6 +370,13 @@ int b2p_segmented_reduce(int dtype, int op, const void *in, const int64_t *offse
   if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_status(e);
   if (total < 0) return B2P_ERR_INVALID_ARG;
+  cs.set_size((size_t)total, (double)total * dtype_size(dtype) + (double)nseg * (acc_size(dtype) + 8));
+  if ((rc = check_extent(in, (size_t)total * dtype_size(dtype))) ||
+      (rc = check_extent(out, (size_t)nseg * acc_size(dtype))) ||
+      (rc = check_extent(offsets, 8 * ((size_t)nseg + 1))) ||
+      (rc = check_offsets(offsets, nseg, (size_t)total, (cudaStream_t)stream)))
+    return rc;
+  if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_SEG_REDUCE, dtype, (size_t)total, nseg, config);
   if (!config_valid(B2P_PRIM_SEG_REDUCE, dtype, config)) return B2P_ERR_INVALID_ARG;
   return launch_segmented(B2P_PRIM_SEG_REDUCE, dtype, op, 1, in, out, offsets, nseg,
@@ -337,9 +384,16 @@ int b2p_segmented_reduce(int dtype, int op, const void *in, const int64_t *offse
                           (cudaStream_t)stream);
 }
 
-int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in, void *out,
-                       const int64_t *offsets, int64_t nseg, const void *init, void *scratch,
-                       size_t scratch_bytes, int config, b2p_stream stream) {
+int b2p_segmented_reduce(int dtype, int op, const void *in, const int64_t *offsets, int64_t nseg,
+                         void *out, const void *init, void *scratch, size_t scratch_bytes,
+                         int config, b2p_stream stream) {
+  CallScope cs("b2p_segmented_reduce", dtype, 0, nseg, 0.0, stream);
+  return cs.done(segmented_reduce_entry(dtype, op, in, offsets, nseg, out, init, scratch, scratch_bytes, config, stream, cs));
+}
+
+static int segmented_scan_entry(int dtype, int op, int inclusive, const void *in, void *out,
+                                const int64_t *offsets, int64_t nseg, const void *init, void *scratch,
+                                size_t scratch_bytes, int config, b2p_stream stream, CallScope &cs) {
   if (!valid_dtype(dtype) || !valid_op(dtype, op) || nseg < 0) return B2P_ERR_INVALID_ARG;
   if (!inclusive && !init) return B2P_ERR_INVALID_ARG;
   if (nseg == 0) return B2P_OK;
@@ -348,7 +402,6 @@ int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in, void *o
   if ((rc = check_ptr(in, dtype_size(dtype))) || (rc = check_ptr(out, acc_size(dtype))) ||
       (rc = check_ptr(offsets, 8)))
     return rc;
-  if (!scratch) return B2P_ERR_SCRATCH;
   int64_t total = 0;
   cudaError_t e = cudaMemcpyAsync(&total, offsets + nseg, sizeof(int64_t), cudaMemcpyDefault,
                                   (cudaStream_t)stream);
@@ -356,11 +409,25 @@ int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in, void *o
   if (e != cudaSuccess) return cuda_status(e);
   if (total < 0) return B2P_ERR_INVALID_ARG;
   if (total == 0) return B2P_OK;
+  cs.set_size((size_t)total, (double)total * (dtype_size(dtype) + acc_size(dtype)) + 8.0 * nseg);
+  if ((rc = check_extent(in, (size_t)total * dtype_size(dtype))) ||
+      (rc = check_extent(out, (size_t)total * acc_size(dtype))) ||
+      (rc = check_extent(offsets, 8 * ((size_t)nseg + 1))) ||
+      (rc = check_offsets(offsets, nseg, (size_t)total, (cudaStream_t)stream)))
+    return rc;
+  if (!scratch) return B2P_ERR_SCRATCH;
   config = resolve(B2P_PRIM_SEG_SCAN, dtype, (size_t)total, nseg, config);
   if (!config_valid(B2P_PRIM_SEG_SCAN, dtype, config)) return B2P_ERR_INVALID_ARG;
   return launch_segmented(B2P_PRIM_SEG_SCAN, dtype, op, inclusive, in, out, offsets, nseg,
                           (size_t)total, init, scratch, scratch_bytes, config,
                           (cudaStream_t)stream);
+}
+
+int b2p_segmented_scan(int dtype, int op, int inclusive, const void *in, void *out,
+                       const int64_t *offsets, int64_t nseg, const void *init, void *scratch,
+                       size_t scratch_bytes, int config, b2p_stream stream) {
+  CallScope cs("b2p_segmented_scan", dtype, 0, nseg, 0.0, stream);
+  return cs.done(segmented_scan_entry(dtype, op, inclusive, in, out, offsets, nseg, init, scratch, scratch_bytes, config, stream, cs));
 }
 
 int b2p_device_error(void *scratch, b2p_stream stream, int clear) {

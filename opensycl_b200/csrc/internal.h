@@ -43,6 +43,43 @@ int cuda_status(cudaError_t e);
 // (B2P_PRIM_MERGE) on n keys of dtype; 0 for other dtypes.
 size_t merge_sort_scratch_bytes(int prim, int dtype, size_t n);
 
+// ------------------------------------------------ logging and checks (log.cu)
+// Log level (B2P_LOG_LEVEL, else ACPP_DEBUG_LEVEL / HIPSYCL_DEBUG_LEVEL;
+// default 2) and one stderr line at `level` (1 error .. 4 verbose).
+int log_level();
+void set_log_level(int level);
+void log_line(int level, const char *fmt, ...);
+// The configuration a call resolved (reported by its call record).
+void note_config(int config);
+// B2P_CHECKED: extents of pointer arguments and segment offsets are checked.
+bool checked_mode();
+int check_extent(const void *p, size_t bytes);
+int check_offsets(const int64_t *offsets, int64_t nseg, size_t total, cudaStream_t st);
+// B2P_SELECTOR: 0 = installed selector table, else heuristic; 1 = heuristic.
+int selector_mode();
+
+// One C-ABI call: an NVTX range over the host call, and its record at log
+// level 3 (4: timed on the stream).  done(status) logs and returns status.
+class CallScope {
+ public:
+  CallScope(const char *op, int dtype, size_t n, int64_t nseg, double bytes, b2p_stream stream);
+  CallScope(const CallScope &) = delete;
+  CallScope &operator=(const CallScope &) = delete;
+  ~CallScope();
+  void set_size(size_t n, double bytes);  // once the element count is known
+  int done(int status);
+
+ private:
+  const char *op_;
+  int dtype_;
+  size_t n_;
+  int64_t nseg_;
+  double bytes_;
+  cudaStream_t st_;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+  bool timed_ = false;
+};
+
 // Device-accessibility and alignment check of a pointer (B2P_OK or
 // B2P_ERR_INVALID_PTR); no CPU fallback.
 int check_pointer(const void *p, size_t align);

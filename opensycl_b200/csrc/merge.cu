@@ -57,13 +57,15 @@ size_t merge_sort_scratch_bytes(int prim, int dtype, size_t n) {
 
 using namespace b2p;
 
-extern "C" int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
-                         void *scratch, size_t scratch_bytes, b2p_stream stream) {
+static int merge_entry(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
+                       void *scratch, size_t scratch_bytes, b2p_stream stream) {
   if (!sortable(dtype)) return dtype == B2P_BF16 ? B2P_ERR_UNSUPPORTED : B2P_ERR_INVALID_ARG;
   if (na + nb == 0) return B2P_OK;
   const size_t es = dtype_size(dtype);
   int rc;
   if ((na && (rc = check_pointer(a, es))) || (nb && (rc = check_pointer(b, es))) || (rc = check_pointer(out, es)))
+    return rc;
+  if ((rc = check_extent(a, na * es)) || (rc = check_extent(b, nb * es)) || (rc = check_extent(out, (na + nb) * es)))
     return rc;
   if (!scratch || scratch_bytes + 256 < merge_sort_scratch_bytes(B2P_PRIM_MERGE, dtype, na + nb) ||
       check_pointer(scratch, 8))
@@ -82,13 +84,14 @@ extern "C" int b2p_merge(int dtype, const void *a, size_t na, const void *b, siz
   }
 }
 
-extern "C" int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
-                        b2p_stream stream) {
+static int sort_entry(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
+                      b2p_stream stream) {
   if (!sortable(dtype)) return dtype == B2P_BF16 ? B2P_ERR_UNSUPPORTED : B2P_ERR_INVALID_ARG;
   if (n <= 1) return B2P_OK;
   const size_t es = dtype_size(dtype);
   int rc = check_pointer(keys, es);
   if (rc) return rc;
+  if ((rc = check_extent(keys, n * es))) return rc;
   if (n > (size_t)merge_tile<long long>()) {
     if (!scratch || scratch_bytes + 256 < merge_sort_scratch_bytes(B2P_PRIM_SORT, dtype, n)) return B2P_ERR_SCRATCH;
     if ((rc = check_pointer(scratch, 256))) return B2P_ERR_SCRATCH;
@@ -102,4 +105,16 @@ extern "C" int b2p_sort(int dtype, void *keys, size_t n, int descending, void *s
   case B2P_F32: return sort_t<float>(keys, n, descending, scratch, scratch_bytes, st);
   default: return sort_t<double>(keys, n, descending, scratch, scratch_bytes, st);
   }
+}
+
+extern "C" int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, void *out, int descending,
+                         void *scratch, size_t scratch_bytes, b2p_stream stream) {
+  CallScope cs("b2p_merge", dtype, na + nb, 0, 2.0 * (double)(na + nb) * dtype_size(dtype), stream);
+  return cs.done(merge_entry(dtype, a, na, b, nb, out, descending, scratch, scratch_bytes, stream));
+}
+
+extern "C" int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
+                        b2p_stream stream) {
+  CallScope cs("b2p_sort", dtype, n, 0, 2.0 * (double)n * dtype_size(dtype), stream);
+  return cs.done(sort_entry(dtype, keys, n, descending, scratch, scratch_bytes, stream));
 }

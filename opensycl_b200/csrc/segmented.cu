@@ -466,6 +466,9 @@ int launch_segmented(int prim, int dtype, int op, int inclusive, const void *in,
 
 struct b2p_plan_s {
   int prim, dtype, op, config;
+  size_t n = 0;       // elements (call records)
+  int64_t nseg = 0;
+  double bytes = 0;   // algorithmic bytes of one launch
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   cudaGraph_t graph = nullptr;
@@ -507,6 +510,9 @@ int b2p_plan_segmented(b2p_plan *plan, int prim, int dtype, int op, const void *
   b2p_plan_s *pl = new b2p_plan_s();
   pl->prim = prim;
   pl->dtype = dtype;
+  pl->n = total_elems;
+  pl->nseg = nseg;
+  pl->bytes = (double)total_elems * dtype_size(dtype) * (prim == B2P_PRIM_SEG_SCAN ? 2 : 1) + 8.0 * nseg;
   pl->op = op;
   pl->config = config;
   pl->scratch_bytes = kScratchPrefix + np * (sizeof(StatusWord) + sizeof(Piece));
@@ -605,8 +611,11 @@ int b2p_segmented_per_call(int prim, int dtype, int op, const void *in, void *ou
 }
 
 int b2p_plan_launch(b2p_plan plan, b2p_stream stream) {
-  if (!plan || !plan->exec) return B2P_ERR_INVALID_ARG;
-  return cuda_status(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
+  CallScope cs("b2p_plan_launch", plan ? plan->dtype : -1, plan ? plan->n : 0, plan ? plan->nseg : 0,
+               plan ? plan->bytes : 0.0, stream);
+  if (!plan || !plan->exec) return cs.done(B2P_ERR_INVALID_ARG);
+  note_config(plan->config);
+  return cs.done(cuda_status(cudaGraphLaunch(plan->exec, (cudaStream_t)stream)));
 }
 
 int b2p_plan_config(b2p_plan plan) { return plan ? plan->config : -1; }

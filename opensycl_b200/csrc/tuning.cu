@@ -49,7 +49,7 @@ int heuristic_config(int prim, int dtype, size_t n, int64_t nseg) {
   case B2P_PRIM_SCAN:
     // pipelined (TMA) kernel from 8 MiB of input on; below that the
     // one-tile-per-block look-back kernel fills the GPU faster
-    if (dtype != B2P_BF16 && n * dtype_size(dtype) >= (8u << 20))
+    if (n * dtype_size(dtype) >= (8u << 20))
       return cfg(1, 256, dtype_size(dtype) == 8 ? 16 : 32);
     return cfg(0, 256, dtype_size(dtype) == 8 ? 16 : 32);
   case B2P_PRIM_COPY_IF:
@@ -227,7 +227,7 @@ int b2p_heuristic_config(int prim, int dtype, size_t n, int64_t nseg) {
 }
 
 int b2p_auto_config(int prim, int dtype, size_t n, int64_t nseg, double cv) {
-  int c = auto_lookup(prim, dtype, n, nseg, cv);
+  int c = selector_mode() == 1 ? -1 : auto_lookup(prim, dtype, n, nseg, cv);
   if (c >= 0 && b2p_config_valid(prim, dtype, c)) return c;
   c = heuristic_config(prim, dtype, n, nseg);
   if (b2p_config_valid(prim, dtype, c)) return c;
