@@ -606,15 +606,16 @@ def measure_ops(C, torch, np, peak, log2n=28, reps=10):
     keys0 = keys0.to(torch.int32)
     ssb = L.b2p_scratch_bytes(C.PRIM_SORT, C.I32, n, 0, C.AUTO)
     sscr = torch.empty(ssb, dtype=torch.uint8, device="cuda")
-    tile = 4096
-    passes = max(0, (n - 1).bit_length() - (tile - 1).bit_length())
-    nbytes = 8 * n * (1 + passes) + (8 * n if passes % 2 else 0)
+    # 2^15 keys and more: the LSD radix sort, 4 digit passes of 8 bits over
+    # int32 keys, each an upsweep read plus a downsweep read and write
+    passes = 4
+    nbytes = 3 * 4 * n * passes
     ms = _time_op(torch, lambda: C.check(L.b2p_sort(C.I32, mo.data_ptr(), n, 0, sscr.data_ptr(), ssb, sh)),
                   reps=reps, flush=None, pre=lambda: mo.copy_(keys0))
     gbs = nbytes / (ms / 1e3) / 1e9
     ops[f"sort_i32_{sz}"] = {"ms": round(ms, 4), "Gkeys/s": round(n / ms / 1e6, 2), "GB/s": round(gbs, 1),
                             "frac_hbm": round(gbs / peak, 4), "bytes": nbytes,
-                            "note": f"random keys; block sort of {tile}-key tiles + {passes} merge passes "
+                            "note": f"random keys; LSD radix sort, {passes} passes of 8 bits "
                                     "(bytes = what those passes move)"}
     del keys0, mo, mscr, sscr
     k = torch.from_numpy(C.synth_fill(4, 5, n, 1.2)).cuda()

@@ -954,10 +954,12 @@ b2p_sycl::event sort(b2p_sycl::queue &q, RandomIt first, RandomIt last, Compare 
     detail::gather_kernel<T><<<detail::copy_grid(n), detail::kGB, 0, st>>>(first, n, keys);
   }
   void *tmp = nullptr;
-  const size_t tmp_bytes = ::b2p::sort_scratch_bytes<T>(n);
+  constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
+  // libb2p's sort (radix for long inputs) sizes its own scratch
+  size_t tmp_bytes = ::b2p::sort_scratch_bytes<T>(n);
+  if constexpr (dt >= 0 && ord != 0) tmp_bytes = b2p_scratch_bytes(B2P_PRIM_SORT, dt, n, 0, B2P_CONFIG_AUTO);
   if (n > (size_t)::b2p::merge_tile<T>()) tmp = q.work_buffer(tmp_bytes);
   int rc;
-  constexpr int dt = detail::sort_dtype<T>(), ord = detail::std_order<Compare>::value;
   if constexpr (dt >= 0 && ord != 0)
     rc = b2p_sort(dt, keys, n, ord == 2, tmp, tmp ? tmp_bytes : 0, (b2p_stream)st);
   else

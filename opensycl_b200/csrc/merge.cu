@@ -1,7 +1,9 @@
-// b2p_merge / b2p_sort: the merge-path merge and the merge sort of
-// b2p_device/merge.cuh for the standard key types, ascending (std::less) or
-// descending (std::greater).
+// b2p_merge / b2p_sort for the standard key types, ascending (std::less) or
+// descending (std::greater): the merge-path merge of b2p_device/merge.cuh,
+// and a sort that is the LSD radix sort of b2p_device/radix.cuh from
+// kRadixMinKeys keys on (below 2^31 keys), the merge sort otherwise.
 #include "b2p_device/merge.cuh"
+#include "b2p_device/radix.cuh"
 #include "internal.h"
 
 namespace b2p {
@@ -26,14 +28,26 @@ int merge_t(const void *a, size_t na, const void *b, size_t nb, void *out, bool 
               : launch_merge(pa, na, pb, nb, po, Less<T>{}, scratch, sb, st);
 }
 
+// Below this many keys one or a few merge-sort launches beat the radix
+// sort's histogram and digit passes.
+constexpr size_t kRadixMinKeys = (size_t)1 << 15;
+
+template <class T>
+bool use_radix(size_t n) {
+  return n >= kRadixMinKeys && n < kRadixMaxKeys;
+}
+
 template <class T>
 size_t scratch_t(int prim, size_t n) {
-  return prim == B2P_PRIM_SORT ? sort_scratch_bytes<T>(n) : merge_scratch_bytes<T>(n);
+  if (prim != B2P_PRIM_SORT) return merge_scratch_bytes<T>(n);
+  return use_radix<T>(n) ? radix_scratch_bytes<T>(n) : sort_scratch_bytes<T>(n);
 }
 
 template <class T>
 int sort_t(void *keys, size_t n, bool desc, void *scratch, size_t sb, cudaStream_t st) {
   T *k = reinterpret_cast<T *>(keys);
+  if (use_radix<T>(n))
+    return launch_radix_sort(k, n, desc, scratch, sb, device_info().sm_count, st);
   return desc ? launch_sort(k, n, Greater<T>{}, scratch, sb, st) : launch_sort(k, n, Less<T>{}, scratch, sb, st);
 }
 

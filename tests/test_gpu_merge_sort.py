@@ -5,7 +5,8 @@ Bar: bit-exact (keys are moved, never computed), including the order of
 keys that compare equal but differ in their bits (-0.0 / +0.0: the stable
 order).  Cases: the known answers of the reference's tests/pstl/merge.cpp
 and sort.cpp (tests/golden/merge_sort_cases.npz), every key type in both
-directions at sizes around the 2048-key tile, ragged and empty inputs,
+directions at sizes around the merge and radix tiles (b2p_sort runs the
+radix sort from 2^15 keys on), ragged and empty inputs, extreme keys,
 duplicates-heavy keys, and at 2^28 keys size-independent properties
 (sorted, the same multiset as the input: the sum of the keys and the
 histogram of their top byte).
@@ -25,7 +26,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mer
 DT = [C.I32, C.I64, C.U32, C.U64, C.F32, C.F64]
 NP = {C.I32: np.int32, C.I64: np.int64, C.U32: np.uint32, C.U64: np.uint64, C.F32: np.float32,
       C.F64: np.float64}
-SIZES = [1, 2, 7, 255, 2047, 2048, 2049, 4096, 3 * 2048 + 17, 100003, (1 << 20) + 5]
+# around the merge sort's 4096-key tiles, the radix sort's start (2^15 keys)
+# and its 8192-key tiles
+SIZES = [1, 2, 7, 255, 2047, 2048, 2049, 4096, 3 * 2048 + 17, 32767, 32768, 5 * 8192, 5 * 8192 + 1, 100003,
+         (1 << 20) + 5]
 
 
 def keys(rng, code, n, dup=False):
@@ -139,3 +143,29 @@ def test_bf16_and_bad_args_are_rejected(dev):
     assert L.b2p_merge(C.I32, a.data_ptr(), 8, a.data_ptr(), 8, o.data_ptr(), 0, None, 0, None) == C.ERR_SCRATCH
     host = np.zeros(8, dtype=np.int32)
     assert L.b2p_sort(C.I32, host.ctypes.data, 8, 0, None, 0, None) == C.ERR_INVALID_PTR
+
+
+@pytest.mark.parametrize("code", DT)
+def test_sort_extreme_and_uniform_keys(dev, code):
+    """Every key the same (one digit value in every radix pass), and the
+    extremes of the type (minimum, maximum, infinities, both zeros) mixed
+    into random keys, in both directions."""
+    rng = np.random.default_rng(300 + code)
+    n = 100003
+    same = np.full(n, 5, dtype=NP[code])
+    t = dev_t(same)
+    C.sort_(t)
+    assert same_bits(t.cpu().numpy(), same)
+    x = keys(rng, code, n)
+    if code in (C.F32, C.F64):
+        ext = np.array([np.inf, -np.inf, 0.0, -0.0, np.finfo(NP[code]).max, np.finfo(NP[code]).min,
+                        np.finfo(NP[code]).tiny, -np.finfo(NP[code]).tiny], dtype=NP[code])
+    else:
+        info = np.iinfo(NP[code])
+        ext = np.array([info.min, info.max, 0, 1, info.max - 1, info.min + 1], dtype=NP[code])
+    idx = rng.integers(0, n, 4000)
+    x[idx] = ext[rng.integers(0, ext.size, idx.size)]
+    for desc in (False, True):
+        t = dev_t(x)
+        C.sort_(t, descending=desc)
+        assert same_bits(t.cpu().numpy(), O.sort(x, desc)), desc
