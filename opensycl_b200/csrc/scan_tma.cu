@@ -248,8 +248,111 @@ __device__ __forceinline__ void tmem_emit(const uint32_t *w, typename P::Acc sta
   }
 }
 
+// Combination of the reducers' per-thread totals inside a tile, done off
+// the reducers' path: the aggregator warp forms the tile total, the emitters
+// the threads' exclusive prefixes.  Compensated sums combine in FP64 (a
+// normalised double-float total converts to double exactly, and a tile's
+// 256 double additions stay far below the sums' error bound); other
+// policies combine their own accumulator.
+template <class P>
+struct TileOps {
+  static constexpr bool kF64 = P::kCompensated;
+  using Acc = typename P::Acc;
+  using Pub = typename std::conditional<kF64, double, Acc>::type;
+  __device__ static Pub identity() {
+    if constexpr (kF64) return 0.0;
+    else return P::identity();
+  }
+  __device__ static Pub combine(Pub a, Pub b) {
+    if constexpr (kF64) return a + b;
+    else return P::combine(a, b);
+  }
+  __device__ static Pub from(Acc a) {
+    if constexpr (kF64) return (double)a.hi + (double)a.lo;
+    else return a;
+  }
+  __device__ static Acc to_acc(Pub v) {
+    if constexpr (kF64) {
+      const float h = (float)v;
+      return DF{h, (float)(v - (double)h)};
+    } else {
+      return v;
+    }
+  }
+};
+
+// Aggregator warp of the TMEM-staged scan, item by item: wait until every
+// reducer warp has parked the tile (slot_ready: one arrival per reducer
+// warp), sum the tile's NC thread totals, publish the aggregate (tile 0: its
+// inclusive prefix) and hand it to the look-back warps (aggr).  Aggregates go
+// out in tile order as soon as tiles are parked, whatever the look-backs are
+// waiting for.  Ends when the reducers have published the item count and it
+// has handled that many items.
+template <class P, class Ops, int NC, bool WIDE>
+__device__ __forceinline__ void scan_aggregator_loop(const TmaParams &p, PipeState &ps,
+                                                     const typename P::Acc *aggs_all,
+                                                     unsigned long long init_bits, unsigned long long epoch_tag,
+                                                     int S) {
+  using TO = TileOps<P>;
+  using V = typename TO::Pub;
+  const int lane = threadIdx.x & 31;
+  RingPos r;
+  for (long long it = 0;; ++it, r.advance(1, S)) {
+    const int s = r.s;
+    int go = 0;
+    if (lane == 0) {
+      uint64_t t0 = 0;
+      for (unsigned k = 0;; ++k) {
+        if (mbar_try_hint(&ps.slot_ready[s], r.ph, 2000)) {
+          go = 1;
+          break;
+        }
+        if (it >= *reinterpret_cast<volatile long long *>(&ps.end_item)) break;
+        if ((k & 7) == 7) {
+          const uint64_t now = globaltimer_ns();
+          if (t0 == 0) {
+            t0 = now;
+          } else if (now - t0 > p.timeout_ns) {
+            record_error(p.hdr, B2P_ERR_TIMEOUT);
+            go = -1;
+            break;
+          }
+        }
+      }
+    }
+    go = __shfl_sync(0xffffffffu, go, 0);
+    if (go <= 0) return;
+    (void)mbar_try(&ps.slot_ready[s], r.ph);  // completed: this lane's acquire of the parked totals
+    const long long tile = ps.tile[s];
+    // the tile total: NC / 32 totals per lane, then a shuffle tree
+    V v = TO::identity();
+#pragma unroll
+    for (int k = 0; k < NC / 32; ++k) v = TO::combine(v, TO::from(aggs_all[(size_t)s * NC + k * 32 + lane]));
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v = TO::combine(v, shfl_xor(v, m));
+    if (lane == 0) {
+      unsigned long long bits;
+      if constexpr (WIDE) bits = F64Ops::pack(v);
+      else bits = publish_value<P, WIDE>(TO::to_acc(v));
+      if (tile != p.stall_tile) {
+        if (tile == 0)
+          st_status(p.status, Ops::pack(Ops::combine(Ops::unpack(init_bits), Ops::unpack(bits))),
+                    epoch_tag | kFlagPrefix);
+        else
+          st_status(p.status + tile, bits, epoch_tag | kFlagAgg);
+      }
+      ps.agg[s] = bits;
+      mbar_arrive(&ps.aggr[s]);
+    }
+    __syncwarp();
+  }
+}
+
+// Threads of the TMEM-staged scan: the pipeline's roles plus the aggregator.
+constexpr int scan_tmem_threads(int nc) { return pipe_threads(nc) + 32; }
+
 template <class P, int NC, int ITEMS, bool WIDE>
-__global__ void __launch_bounds__(pipe_threads(NC), 1)
+__global__ void __launch_bounds__(scan_tmem_threads(NC), 1)
     scan_tmem_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
                      TmaParams p) {
   using In = typename P::In;
@@ -271,9 +374,9 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   extern __shared__ char smem_raw[];
   char *smem = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   char *obase = smem + p.out_base;
-  Acc *texcl_all = reinterpret_cast<Acc *>(smem + p.texcl_base);
+  Acc *aggs_all = reinterpret_cast<Acc *>(smem + p.texcl_base);  // per slot: each reducer thread's total
   __shared__ __align__(8) PipeState ps;
-  __shared__ Acc s_warp[32];
+  __shared__ typename TileOps<P>::Pub s_warp[32];
   __shared__ int s_go[2];
 
   const int warp = threadIdx.x >> 5;
@@ -324,25 +427,14 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
       tmem_st16(ta, w);
       if constexpr (kCols == 32) tmem_st16(ta + 16, w + 16);
-      Acc tile_agg;
-      texcl_all[(size_t)rs.s * NC + t] = group_exclusive_scan_1bar<AccOps<P>, NC>(agg, s_warp, &tile_agg, t, 1);
-      if (t == 0) {  // the aggregate goes out before the slot is complete
-        const unsigned long long bits = publish_value<P, WIDE>(tile_agg);
-        if (tile != p.stall_tile) {
-          if (tile == 0)
-            st_status(p.status, Ops::pack(Ops::combine(Ops::unpack(init_bits), Ops::unpack(bits))),
-                      epoch_tag | kFlagPrefix);
-          else
-            st_status(p.status + tile, bits, epoch_tag | kFlagAgg);
-        }
-        ps.tile[rs.s] = tile;
-        ps.agg[rs.s] = bits;
-        mbar_arrive(&ps.aggr[rs.s]);
-      }
+      // the tile total and the threads' prefixes are formed by the aggregator
+      // warp and the emitters: the reducers only park the thread totals
+      aggs_all[(size_t)rs.s * NC + t] = agg;
+      if (t == 0) ps.tile[rs.s] = tile;
       tmem_wait_st();
       tmem_fence_before();
       __syncwarp();
-      if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);  // this warp's slot columns and prefixes
+      if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);  // this warp's slot columns and totals
     }
     if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
   } else if (warp < 2 * NC / 32) {
@@ -353,8 +445,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
     RingPos rs, ro;
     for (long long it = 0;; ++it, rs.advance(1, SL), ro.advance(1, SO)) {
       if (t == 0) {
+        // the carry is ready only after every reducer warp parked the tile
         int go = emitter_wait(p, ps, rs, it);
-        if (go > 0 && !mbar_wait(&ps.slot_ready[rs.s], rs.ph, p.timeout_ns)) go = -1;
         if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
         if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         if (go == 0) {
@@ -374,7 +466,13 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       const uint32_t ta = tcol + (uint32_t)(rs.s * kSlotCols);
       if constexpr (kCols == 32) tmem_load32(ta, w);
       else tmem_load16(ta, w);
-      const Acc start = start_value<P, WIDE>(ps.carry[rs.s], texcl_all[(size_t)rs.s * NC + t]);
+      using TO = TileOps<P>;
+      typename TO::Pub tile_total;
+      const typename TO::Pub ex =
+          group_exclusive_scan_1bar<TO, NC>(TO::from(aggs_all[(size_t)rs.s * NC + t]), s_warp, &tile_total, t, 2);
+      Acc start;
+      if constexpr (WIDE && TO::kF64) start = TO::to_acc(F64Ops::unpack(ps.carry[rs.s]) + ex);
+      else start = start_value<P, WIDE>(ps.carry[rs.s], TO::to_acc(ex));
       tmem_fence_before();
       __syncwarp();
       if ((t & 31) == 0) mbar_arrive(&ps.slot_free[rs.s]);  // slot, carry and prefixes read
@@ -396,6 +494,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
     lookback_loop<Ops>(p, ps, warp - 2 * NC / 32, init_bits, epoch_tag, SL);
   } else if (warp == 2 * NC / 32 + kLookWarps) {
     if ((threadIdx.x & 31) == 0) producer_loop(&tin, p, ps, smem, kRows, kBox, ps.tile_in);
+  } else if (warp == 2 * NC / 32 + kLookWarps + 2) {
+    scan_aggregator_loop<P, Ops, NC, WIDE>(p, ps, aggs_all, init_bits, epoch_tag, SL);
   } else {
     // ---------------------------------------------------------- store warp
     if ((threadIdx.x & 31) == 0) {
@@ -646,7 +746,7 @@ int launch_tmem_shape(TmaParams &p, const CUtensorMap &tin, const CUtensorMap &t
     const size_t smem = p.texcl_base + (size_t)p.slots * NC * sizeof(typename P::Acc) + 1024;
     int rc = ensure_dynamic_smem((const void *)kfn, smem);
     if (rc) return rc;
-    const int threads = pipe_threads(NC);
+    const int threads = scan_tmem_threads(NC);
     if (occupancy((const void *)kfn, threads, smem) < 1) return B2P_ERR_UNSUPPORTED;
     const int grid = (int)std::min<long long>(p.ntiles, (long long)device_info().sm_count);
     kfn<<<grid, threads, smem, st>>>(tin, tout, p);
