@@ -306,6 +306,45 @@ int b2p_merge(int dtype, const void *a, size_t na, const void *b, size_t nb, voi
 int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, size_t scratch_bytes,
              b2p_stream stream);
 
+/* ------------------------------------------------------------ sharded
+ * One logical array spread over the ranks of an NCCL communicator (one
+ * process or thread per GPU, rank r holding the r-th contiguous shard).  The
+ * reference runs every algorithm on one sycl::queue, i.e. one device
+ * (algorithms/numeric.hpp, algorithm.hpp); these calls extend its reduce
+ * (numeric.hpp:170-236) and scans (numeric.hpp:251-327) across devices with
+ * a single exchange: each rank's shard partial (16 bytes) is all-gathered
+ * on `stream` and combined in rank order on the host, so every rank gets the
+ * same bits.  `nccl_comm` is an ncclComm_t of the libnccl.so.2 loaded in
+ * the process (libb2p resolves NCCL's functions there and does not link
+ * it).  The calls return after their work is complete (they synchronise
+ * `stream`).  scratch: b2p_sharded_scratch_bytes(dtype, n, world) bytes,
+ * zero-filled once (b2p_scratch_init), not shared with overlapping calls.
+ * B2P_ERR_UNSUPPORTED when no libnccl.so.2 can be loaded. */
+size_t b2p_sharded_scratch_bytes(int dtype, size_t n, int world);
+
+/* *out (device, accumulation type) = init op (the reduction of every rank's
+ * shard); init NULL: nothing folded in.  Integers wrap; float partials are
+ * combined in double.  A rank may hold an empty shard (n == 0); when every
+ * shard is empty and init is NULL, *out is left untouched. */
+int b2p_sharded_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
+                       void *scratch, size_t scratch_bytes, int config, void *nccl_comm, b2p_stream stream);
+
+/* This rank's part of the inclusive (or exclusive) scan of the concatenated
+ * shards: out[i] as the one-device scan of the whole array would give it.
+ * The local scan runs once, with the combination of init and the totals of
+ * the ranks before as its init.  Exclusive scans need init. */
+int b2p_sharded_scan(int dtype, int op, int inclusive, const void *in, void *out, size_t n, const void *init,
+                     void *scratch, size_t scratch_bytes, int config, void *nccl_comm, b2p_stream stream);
+
+/* Host-side combination of exchanged partials, for hosts that move them
+ * with their own transport: *result = init op values[0] op ... op
+ * values[count - 1] (HOST memory; entries of the accumulation type, `stride`
+ * bytes apart; init NULL: nothing folded in).  The rank-order combination
+ * b2p_sharded_reduce and b2p_sharded_scan (carry = the first `rank` totals)
+ * use.  B2P_ERR_INVALID_ARG when count == 0 and init is NULL. */
+int b2p_shard_combine(int dtype, int op, const void *values, int count, size_t stride, const void *init,
+                      void *result);
+
 /* Log level of the library's stderr records (0 none, 1 errors, 2 warnings,
  * 3 one line per call, 4 each call also timed on its stream, which makes
  * the call wait for its work).  Initialised from B2P_LOG_LEVEL, else

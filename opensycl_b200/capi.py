@@ -86,6 +86,12 @@ def _declare(L):
         "b2p_histogram_u8": ([vp, sz, vp, i, i, vp], i),
         "b2p_merge": ([i, vp, sz, vp, sz, vp, i, vp, sz, vp], i),
         "b2p_sort": ([i, vp, sz, i, vp, sz, vp], i),
+        "b2p_sharded_scratch_bytes": ([i, sz, i], sz),
+        "b2p_sharded_reduce": ([i, i, vp, sz, vp, vp, vp, sz, i, vp, vp], i),
+        "b2p_sharded_scan": ([i, i, i, vp, vp, sz, vp, vp, sz, i, vp, vp], i),
+        "b2p_shard_combine": ([i, i, vp, i, sz, vp, vp], i),
+        "b2p_log_level": ([], i),
+        "b2p_set_log_level": ([i], None),
         "b2p_segmented_reduce": ([i, i, vp, vp, i64, vp, vp, vp, sz, i, vp], i),
         "b2p_segmented_scan": ([i, i, i, vp, vp, vp, i64, vp, vp, sz, i, vp], i),
         "b2p_segmented_per_call": ([i, i, i, vp, vp, vp, i64, vp, sz, i, vp], i),

@@ -62,3 +62,61 @@ def test_sharded_two_ranks_one_gpu():
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     mp.spawn(_worker, args=(2, port), nprocs=2, join=True)
+
+
+def _nccl_single_rank_comm():
+    """A one-rank NCCL communicator on the current device, from the
+    libnccl.so.2 of this process (the one libb2p resolves NCCL in)."""
+    import ctypes
+
+    class UniqueId(ctypes.Structure):
+        _fields_ = [("internal", ctypes.c_char * 128)]
+
+    lib = ctypes.CDLL("libnccl.so.2")
+    uid = UniqueId()
+    assert lib.ncclGetUniqueId(ctypes.byref(uid)) == 0
+    comm = ctypes.c_void_p()
+    lib.ncclCommInitRank.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, UniqueId, ctypes.c_int]
+    assert lib.ncclCommInitRank(ctypes.byref(comm), 1, uid, 0) == 0
+    return lib, comm
+
+
+@pytest.mark.gpu
+def test_sharded_c_abi_single_rank(dev):
+    """b2p_sharded_reduce / b2p_sharded_scan through an NCCL communicator of
+    one rank (this run has one GPU): the exchange path (local partial,
+    all-gather, host combination) against b2p_reduce / b2p_scan; the carry
+    logic for more ranks is b2p_shard_combine, tested on the host."""
+    import ctypes
+    import torch
+    torch.cuda.set_device(0)
+    torch.zeros(1, device="cuda")
+    lib, comm = _nccl_single_rank_comm()
+    try:
+        L = C.lib()
+        sh = C._stream(None)
+        rng = np.random.default_rng(3)
+        for code, x in ((C.I64, torch.from_numpy(rng.integers(-1000, 1000, (1 << 20) + 7)).cuda()),
+                        (C.F32, torch.from_numpy(rng.standard_normal((1 << 20) + 7).astype(np.float32)).cuda())):
+            n = x.numel()
+            sb = L.b2p_sharded_scratch_bytes(code, n, 1)
+            scratch = torch.zeros(sb, dtype=torch.uint8, device="cuda")
+            out = torch.zeros(1, dtype=x.dtype, device="cuda")
+            init = np.array([5], dtype=np.int64 if code == C.I64 else np.float32)
+            ip = init.ctypes.data_as(ctypes.c_void_p)
+            assert L.b2p_sharded_reduce(code, C.SUM, x.data_ptr(), n, out.data_ptr(), ip, scratch.data_ptr(), sb,
+                                        C.AUTO, comm, sh) == C.OK
+            ref = C.reduce(x, "sum", init=init[0].item())
+            torch.cuda.synchronize()
+            if code == C.I64:
+                assert out.item() == ref.item()
+            else:
+                assert abs(out.item() - ref.item()) <= 1e-6 * abs(ref.item()) + 1e-3
+            y = torch.empty_like(x)
+            assert L.b2p_sharded_scan(code, C.SUM, 1, x.data_ptr(), y.data_ptr(), n, None, scratch.data_ptr(), sb,
+                                      C.AUTO, comm, sh) == C.OK
+            yr = C.scan(x, True, "sum")
+            torch.cuda.synchronize()
+            assert torch.equal(y, yr)
+    finally:
+        lib.ncclCommDestroy(comm)

@@ -141,3 +141,55 @@ def test_carry_and_combine_wrap():
     assert S.shard_carry(C.U32, "max", [5, 9, 2], 3, None) == 9
     assert S._from_bits(C.F32, S._to_bits(C.F32, 0.1)) == 0.1
     assert S._from_bits(C.U64, S._to_bits(C.U64, np.uint64(2 ** 63 + 5))) == np.uint64(2 ** 63 + 5)
+
+
+# ----------------------------------------------- C-ABI host combination
+# b2p_shard_combine is the rank-order combination that b2p_sharded_reduce
+# and b2p_sharded_scan apply to the gathered partials (a C/C++ host with its
+# own transport calls it directly); it must agree with the Python layer's
+# combine / shard_carry, integer wrap-around included.
+
+import ctypes  # noqa: E402
+
+_NP = {C.I32: np.int32, C.I64: np.int64, C.U32: np.uint32, C.U64: np.uint64, C.F32: np.float32, C.F64: np.float64}
+
+
+def _combine_c(code, op, values, init):
+    L = C.lib()
+    vals = np.ascontiguousarray(values, dtype=_NP[code])
+    res = np.zeros(1, dtype=_NP[code])
+    ip = None
+    if init is not None:
+        ib = np.array([init], dtype=_NP[code])
+        ip = ib.ctypes.data_as(ctypes.c_void_p)
+    rc = L.b2p_shard_combine(code, op, vals.ctypes.data_as(ctypes.c_void_p) if vals.size else None, vals.size,
+                             vals.itemsize, ip, res.ctypes.data_as(ctypes.c_void_p))
+    return rc, res[0]
+
+
+@pytest.mark.parametrize("code", [C.I32, C.I64, C.U32, C.U64, C.F32, C.F64])
+@pytest.mark.parametrize("op", [C.SUM, C.PROD, C.MIN, C.MAX, C.AND, C.OR, C.XOR])
+def test_shard_combine_matches_python_layer(code, op):
+    if code in (C.F32, C.F64) and op > C.MAX:
+        assert _combine_c(code, op, [1, 2], 0)[0] == C.ERR_INVALID_ARG
+        return
+    rng = np.random.default_rng(code * 10 + op)
+    if code in (C.F32, C.F64):
+        vals = rng.standard_normal(7).astype(_NP[code])
+        init = 0.5
+    else:
+        info = np.iinfo(_NP[code])
+        vals = rng.integers(info.min, info.max, 7, dtype=_NP[code], endpoint=True)  # sums and products wrap
+        init = 3
+    for rank in range(len(vals) + 1):
+        rc, got = _combine_c(code, op, vals[:rank], init)
+        assert rc == C.OK
+        want = S.shard_carry(code, op, list(vals), rank, _NP[code](init))
+        if code == C.F32:
+            assert got == np.float32(want)
+        else:
+            assert got == _NP[code](want), (rank, got, want)
+    # no init: the first value starts the fold; nothing to fold is an error
+    rc, got = _combine_c(code, op, vals[:3], None)
+    assert rc == C.OK and got == _NP[code](S.shard_carry(code, op, list(vals[1:]), 2, vals[0]))
+    assert _combine_c(code, op, vals[:0], None)[0] == C.ERR_INVALID_ARG
