@@ -101,12 +101,14 @@ inline size_t radix_scratch_bytes(size_t n) {
   return radix_layout<T>(n, 256).total + 256;
 }
 
-// Lanes of the warp whose 9-bit label (a digit, or 256 for a key past the
-// end) equals this lane's: one ballot per label bit.
+// Lanes of the warp whose label (a digit, or 256 for a key past the end)
+// equals this lane's: one ballot per label bit (BITS = 8 when every key of
+// the round is real, 9 otherwise).
+template <int BITS>
 __device__ __forceinline__ unsigned radix_peers(unsigned label) {
   unsigned peers = 0xffffffffu;
 #pragma unroll
-  for (int b = 0; b < kRadixBits + 1; ++b) {
+  for (int b = 0; b < BITS; ++b) {
     const bool bit = (label >> b) & 1u;
     const unsigned m = __ballot_sync(0xffffffffu, bit);
     peers &= bit ? m : ~m;
@@ -237,7 +239,8 @@ __global__ void __launch_bounds__(kRadixThreads, kRadixBlocksPerSm)
     for (int r = 0; r < kRadixItems; ++r) {
       const int j = wbase + r * 32 + lane;
       const unsigned d = j < count ? RadixKey<T>::digit(key[r], desc, pass) : (unsigned)kRadixBins;
-      const unsigned peers = radix_peers(d);
+      // a full tile has no key past the end: the 9th label bit is always 0
+      const unsigned peers = count == kRadixTile ? radix_peers<kRadixBits>(d) : radix_peers<kRadixBits + 1>(d);
       const unsigned base = wh[d];
       rd[r] = ((base + (unsigned)__popc(peers & lt)) << 9) | d;
       __syncwarp();

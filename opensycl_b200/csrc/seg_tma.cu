@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
   constexpr int kWorkWarps = REDUCE ? kGroups * NC / 32 : 2 * NC / 32;
   __shared__ Pair s_warp_g[kGroups][32];
   __shared__ Acc s_acc_g[kGroups][32];  // clean tiles: warp totals (reduce) or the scan's warp values
+  __shared__ double s_dbl_g[kGroups][32];  // clean tiles of a compensated reduce: FP64 warp totals
   __shared__ int s_go[kGroups > 2 ? kGroups : 2];  // [g]: reducer group g; [1] of a scan: the emitters
   __shared__ int s_entering_end_g[kGroups];
   __shared__ long long s_stop[kGroups];  // reduce: the item at which each group met the end
@@ -192,13 +193,19 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
       // this thread's elements [e0, e0 + lim) of the tile (lim <= 0: none)
       const int e0 = t * ITEMS;
       const int lim = min(ITEMS, count - e0);
-      const int i0 = B.lower(e0);
+      // A clean tile has no segment boundary inside it (a reduce: none at
+      // positions 0 .. count, a scan: no head before count); every tile
+      // inside a long segment is clean.  It needs no segmented operator:
+      // its aggregate is the plain combination of the thread totals, and no
+      // thread has a head or an end to find.
+      const bool clean = m >= 1 && (REDUCE ? B.at(0) > count : B.at(0) >= count);
+      const int i0 = clean ? 0 : B.lower(e0);
       // heads: bit j = a segment starts at e0 + j; ends: bit j = one ends at
       // e0 + j.  Boundaries that share a position with the next one start
       // empty segments (a reduce gives them init), and so does every
       // boundary below nseg at the end of the data.
       unsigned heads = 0, ends = 0;
-      if (lim > 0) {
+      if (lim > 0 && !clean) {
         for (int i = i0; i < m; ++i) {
           const long long at = B.at(i);
           const int r = (int)(at - e0);
@@ -222,11 +229,6 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
       Acc r_end = P::identity();
       uint32_t w[kCols];
       constexpr int IPV = 16 / (int)sizeof(In), VPT = ITEMS / IPV, WPO = (int)sizeof(Out) / 4;
-      // A clean tile has no segment boundary inside it (a reduce: none at
-      // positions 0 .. count, a scan: no head before count); every tile
-      // inside a long segment is clean.  It needs no segmented operator:
-      // its aggregate is the plain combination of the thread totals.
-      const bool clean = m >= 1 && (REDUCE ? B.at(0) > count : B.at(0) >= count);
       if (REDUCE && heads == 0 && ends == 0) {
         // a reduce, no segment starts or ends here: only the thread total
         // matters, folded in kChains independent chains (element j to chain
@@ -348,7 +350,20 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
       }
       if (clean) {
         Acc tile_tot;
-        if constexpr (REDUCE) {
+        if constexpr (REDUCE && P::kCompensated) {
+          // the double-float thread totals combine in FP64: exact conversions,
+          // one add per shuffle step instead of a double-float add
+          double d = (double)run.hi + (double)run.lo;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+          if ((t & 31) == 0) s_dbl_g[g][t >> 5] = d;
+          bar_named(gbar, NC);
+          double sum = s_dbl_g[g][0];
+#pragma unroll
+          for (int w = 1; w < NC / 32; ++w) sum += s_dbl_g[g][w];
+          const float h = (float)sum;
+          tile_tot = Acc{h, (float)(sum - (double)h)};
+        } else if constexpr (REDUCE) {
           const Acc wt = warp_allreduce<P>(run);
           if ((t & 31) == 0) s_acc[t >> 5] = wt;
           bar_named(gbar, NC);
