@@ -116,7 +116,8 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
   __shared__ int s_go[2];
 
   const int warp = threadIdx.x >> 5;
-  tmem_pipe_init(ps, p, NC / 32);
+  // aggr completes when every reducer warp has parked its part of the tile
+  tmem_pipe_init(ps, p, NC / 32, NC / 32);
   if (warp == 0) {
     __syncwarp();
     tmem_alloc(&ps.tmem_base, 512);
@@ -174,18 +175,18 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
       unsigned kept32;
       const unsigned ex = count_scan_1bar<NC>((unsigned)__popc(keep), s_cnt, &kept32, t, 1);
       const unsigned long long tile_kept = kept32;
-      texcl_all[(size_t)rs.s * NC + t] = (uint16_t)ex;
-      keep_all[(size_t)rs.s * NC + t] = keep;
-      tmem_wait_st();
-      tmem_fence_before();
-      bar_named(1, NC);  // slot, keep masks and offsets complete
-      if (t == 0) {
+      if (t == 0) {  // the kept count goes out as soon as the count scan knows it
         if (tile != p.stall_tile)
           st_status(p.status + tile, tile_kept, epoch_tag | (tile == 0 ? kFlagPrefix : kFlagAgg));
         ps.tile[rs.s] = tile;
         ps.agg[rs.s] = tile_kept;
-        mbar_arrive(&ps.aggr[rs.s]);
       }
+      texcl_all[(size_t)rs.s * NC + t] = (uint16_t)ex;
+      keep_all[(size_t)rs.s * NC + t] = keep;
+      tmem_wait_st();
+      tmem_fence_before();
+      __syncwarp();
+      if ((t & 31) == 0) mbar_arrive(&ps.aggr[rs.s]);  // this warp's slot columns, masks and offsets
     }
     if (t == 0) *reinterpret_cast<volatile long long *>(&ps.end_item) = it;
   } else if (warp < 2 * NC / 32) {
@@ -199,9 +200,12 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
         if (go > 0 && !mbar_wait(&ps.out_empty[ro.s], ro.ph ^ 1u, p.timeout_ns)) go = -1;
         if (go < 0) record_error(p.hdr, B2P_ERR_TIMEOUT);
         if (go == 0) {
+          // end the store warp and the look-back warps (waiting on items it ..
+          // it + kLookWarps - 1, each barrier completing after NC / 32 arrivals)
           mbar_arrive(&ps.emitted[ro.s]);
           RingPos r = rs;
-          for (int j = 0; j < kLookWarps; ++j, r.advance(1, SL)) mbar_arrive(&ps.aggr[r.s]);
+          for (int j = 0; j < kLookWarps; ++j, r.advance(1, SL))
+            for (int k = 0; k < NC / 32; ++k) mbar_arrive(&ps.aggr[r.s]);
         }
         s_go[1] = go;
       }

@@ -498,14 +498,15 @@ constexpr int tmem_cols() {
 // Thread 0: barriers of the three rings (input stages, TMEM slots, output
 // stages) and the launch epoch.  Reducer and emitter warps arrive one by one
 // on the barriers that hand back input stages and slots.
-__device__ __forceinline__ void tmem_pipe_init(PipeState &ps, const TmaParams &p, unsigned group_warps) {
+__device__ __forceinline__ void tmem_pipe_init(PipeState &ps, const TmaParams &p, unsigned group_warps,
+                                               unsigned aggr_count = 1) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < p.stages; ++i) {
       mbar_init(&ps.full[i], 1);
       mbar_init(&ps.empty[i], group_warps);
     }
     for (int i = 0; i < p.slots; ++i) {
-      mbar_init(&ps.aggr[i], 1);
+      mbar_init(&ps.aggr[i], aggr_count);
       mbar_init(&ps.cready[i], 1);
       mbar_init(&ps.slot_free[i], group_warps);
       mbar_init(&ps.slot_ready[i], group_warps);
