@@ -169,3 +169,20 @@ def test_sort_extreme_and_uniform_keys(dev, code):
         t = dev_t(x)
         C.sort_(t, descending=desc)
         assert same_bits(t.cpu().numpy(), O.sort(x, desc)), desc
+
+
+def test_sort_largest_radix_input(dev):
+    """2^31 - 5 int32 keys (8 GiB), just below the radix sort's 2^31 limit of
+    32-bit output slots: sorted, and the same multiset (sum of the keys and
+    counts of the top byte)."""
+    n = (1 << 31) - 5
+    g = torch.Generator(device="cuda").manual_seed(9)
+    x = torch.randint(-(1 << 31), (1 << 31) - 1, (n,), generator=g, device="cuda", dtype=torch.int32)
+    s0 = int(torch.sum(x, dtype=torch.int64))
+    h0 = torch.bincount(((x >> 24) & 0xFF).to(torch.int32), minlength=256)
+    C.sort_(x)
+    assert bool((x[1:] >= x[:-1]).all())
+    assert int(torch.sum(x, dtype=torch.int64)) == s0
+    assert torch.equal(torch.bincount(((x >> 24) & 0xFF).to(torch.int32), minlength=256), h0)
+    del x
+    torch.cuda.empty_cache()
