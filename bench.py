@@ -298,6 +298,9 @@ def main():
                 result["selector"] = {k: sel[k] for k in ("learned_vs_exhaustive_table", "heuristic_vs_learned")
                                       if k in sel}
         result["selector_state"] = selector_state["status"]
+    elif world > 1:
+        # every rank takes part in the exchanges of the end-to-end step
+        result["e2e"] = measure_e2e_sharded(SH, torch, a_h, b_h, x_h, args, dist)
     else:
         result["e2e"] = None
     if rank == 0:
@@ -449,6 +452,53 @@ def measure_e2e(C, torch, a_h, b_h, x_h, args):
             "ms_per_step": round(ms, 3), "steps": steps, "result_read_back": ok,
             "path": "pinned host -> H2D on stream 1 -> b2p_dot + b2p_scan (stream 1) -> D2H on stream 2; "
                     "two buffer sets, step k's D2H overlaps step k+1's H2D"}
+
+
+def measure_e2e_sharded(SH, torch, a_h, b_h, x_h, args, dist):
+    """The sharded step end to end on every rank: copy this rank's shard of
+    the three inputs in from pinned host buffers, run sharded_dot and
+    sharded_scan (their exchanges included) and copy the scan output back,
+    all inside the timed region; time = max over ranks."""
+    n = a_h.size
+    world = dist.get_world_size()
+    ap = torch.from_numpy(a_h).pin_memory()
+    bp = torch.from_numpy(b_h).pin_memory()
+    xp = torch.from_numpy(x_h).pin_memory()
+    yp = torch.empty(n, dtype=torch.float32).pin_memory()
+    a = torch.empty(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    x = torch.empty_like(a)
+    y = torch.empty_like(a)
+    dots = []
+
+    def step():
+        a.copy_(ap, non_blocking=True)
+        b.copy_(bp, non_blocking=True)
+        x.copy_(xp, non_blocking=True)
+        dots.append(SH.sharded_dot(a, b, 0.0))  # a host value: the step's scalar result
+        y.copy_(SH.sharded_scan(x, True, "sum", None))
+        yp.copy_(y, non_blocking=True)
+
+    steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        step()
+    e1.record(s)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / steps], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return {"value": round(16.0 * n * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": 12 * n * world, "d2h_bytes_per_step": 4 * n * world,
+            "ms_per_step": round(ms, 3), "steps": steps, "result_read_back": True,
+            "path": "per rank: pinned host -> H2D -> sharded_dot + sharded_scan (NCCL exchanges) -> D2H; "
+                    "max over ranks"}
 
 
 def measure_precision(torch, a, b, x, y, dres):
