@@ -161,6 +161,9 @@ def main():
                     help="elements per array of the per-primitive table (below 28: no 2^24, segmented "
                          "or selector entries; small cases for profiling)")
     ap.add_argument("--ops-reps", type=int, default=10, help="timed launches per primitive")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend for N > 1 (gloo: a functional check of the sharded path, "
+                         "ranks may share a GPU; not a measurement)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -180,13 +183,13 @@ def main():
     from opensycl_b200 import capi as C
     from opensycl_b200 import sharded as SH
 
-    torch.cuda.set_device(local)
+    torch.cuda.set_device(local % max(torch.cuda.device_count(), 1))
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120))
 
     def barrier():
         if dist is not None:
@@ -238,7 +241,7 @@ def main():
         barrier()
     ms = start.elapsed_time(end)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda")
+        t = torch.tensor([ms], device="cuda" if args.dist_backend == "nccl" else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     dot_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
@@ -255,7 +258,8 @@ def main():
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms, dom_bytes = kern[dom]
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = read_traffic().get("scan_f32" if dom.startswith("scan") else "dot_f32")
+    # the committed DRAM-traffic figures are per launch at 2^28 elements
+    traffic = read_traffic().get("scan_f32" if dom.startswith("scan") else "dot_f32") if args.log2n == 28 else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic[0] if traffic else None,
@@ -491,14 +495,14 @@ def measure_e2e_sharded(SH, torch, a_h, b_h, x_h, args, dist):
         step()
     e1.record(s)
     torch.cuda.synchronize()
-    t = torch.tensor([e0.elapsed_time(e1) / steps], device="cuda")
+    t = torch.tensor([e0.elapsed_time(e1) / steps], device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     return {"value": round(16.0 * n * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": 12 * n * world, "d2h_bytes_per_step": 4 * n * world,
             "ms_per_step": round(ms, 3), "steps": steps, "result_read_back": True,
-            "path": "per rank: pinned host -> H2D -> sharded_dot + sharded_scan (NCCL exchanges) -> D2H; "
-                    "max over ranks"}
+            "path": f"per rank: pinned host -> H2D -> sharded_dot + sharded_scan ({dist.get_backend()} exchanges) "
+                    "-> D2H; max over ranks"}
 
 
 def measure_precision(torch, a, b, x, y, dres):
