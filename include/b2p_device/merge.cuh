@@ -97,29 +97,35 @@ __device__ __forceinline__ long long merge_path_warp(IdxA a, long long na, IdxB 
 // read and write 32 different banks.
 __device__ __forceinline__ int spad(int i) { return i + (i >> 5); }
 __host__ __device__ constexpr int spad_size(int n) { return n + n / 32; }
+// Shared slots of a padded tile of n keys plus the spare slot one past it
+// (read, never used, by merge_serial when a side ends at the tile's end).
+__host__ __device__ constexpr int spad_alloc(int n) { return spad_size(n) + 1; }
 
 // Serial stable merge of ITEMS outputs starting at a[ia], b[ib] of the two
 // ranges s[pad(a0 + i)] and s[pad(b0 + i)] of one padded shared array
 // into out[]; the current key of each range stays in a register, and each
 // output costs one shared load, without branches (the warp's threads take
 // different sides).  Outputs past the end of both ranges are left
-// unspecified.  Reads only slots a0 + [0, na), b0 + [0, nb) and slot 0,
-// which stands in for the next key of an exhausted side (its value is
-// never used).
+// unspecified.  The second range follows the first (b0 >= a0 + na), and
+// reads stay in slots a0 .. b0 + nb: one past the end of a side is the
+// first slot of the next range or, past the tile, the array's spare last
+// slot (kept by spad_alloc); once both sides are exhausted the a-side index,
+// which keeps counting, is held at b0 + nb.  Keys read past a side's end
+// are never compared or used.
 template <class T, int ITEMS, class Comp>
 __device__ __forceinline__ void merge_serial(const T *s, int a0, int ia, int na, int b0, int ib, int nb,
                                              T (&out)[ITEMS], const Comp &comp) {
-  T va = s[spad(ia < na ? a0 + ia : 0)];
-  T vb = s[spad(ib < nb ? b0 + ib : 0)];
+  const int end = b0 + nb;
+  T va = s[spad(a0 + ia)];
+  T vb = s[spad(b0 + ib)];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
     const bool take_b = ib < nb && (ia >= na || comp(vb, va));
     out[k] = take_b ? vb : va;
     ia += take_b ? 0 : 1;
-    ib += take_b ? 1 : 0;
-    // the next key of the side just taken
-    const int nxt = take_b ? (ib < nb ? b0 + ib : 0) : (ia < na ? a0 + ia : 0);
-    const T v = s[spad(nxt)];
+    ib += take_b ? 1 : 0;  // ib <= nb: b is taken only while ib < nb
+    // the next key of the side just taken (one past its end when exhausted)
+    const T v = s[spad(take_b ? b0 + ib : min(a0 + ia, end))];
     vb = take_b ? v : vb;
     va = take_b ? va : v;
   }
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long l
                                                               T *out, long long run, const long long *splits,
                                                               Comp comp) {
   constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
-  __shared__ T s_in[spad_size(kMergeTile)];
+  __shared__ T s_in[spad_alloc(kMergeTile)];
   const long long total = PAIRS ? na : na + nb;
   const long long d0 = (long long)blockIdx.x * kMergeTile;
   if (d0 >= total) return;
@@ -236,8 +242,8 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(const T *a, long l
 template <class T, class Comp>
 __global__ void __launch_bounds__(kMergeThreads) block_sort_kernel(T *keys, long long n, Comp comp) {
   constexpr int kMergeItems = merge_items<T>(), kMergeTile = merge_tile<T>();
-  __shared__ T s_a[spad_size(kMergeTile)];
-  __shared__ T s_b[spad_size(kMergeTile)];
+  __shared__ T s_a[spad_alloc(kMergeTile)];
+  __shared__ T s_b[spad_alloc(kMergeTile)];
   const long long t0 = (long long)blockIdx.x * kMergeTile;
   const int cnt = (int)min((long long)kMergeTile, n - t0);
   if (cnt == kMergeTile) {
