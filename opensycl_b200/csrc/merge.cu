@@ -40,14 +40,18 @@ bool use_radix(size_t n) {
 template <class T>
 size_t scratch_t(int prim, size_t n) {
   if (prim != B2P_PRIM_SORT) return merge_scratch_bytes<T>(n);
-  return use_radix<T>(n) ? radix_scratch_bytes<T>(n) : sort_scratch_bytes<T>(n);
+  // the radix sort's need, or the merge sort's, whichever is larger (a
+  // radix sort the device cannot run falls back to the merge sort)
+  return use_radix<T>(n) ? std::max(radix_scratch_bytes<T>(n), sort_scratch_bytes<T>(n)) : sort_scratch_bytes<T>(n);
 }
 
 template <class T>
 int sort_t(void *keys, size_t n, bool desc, void *scratch, size_t sb, cudaStream_t st) {
   T *k = reinterpret_cast<T *>(keys);
-  if (use_radix<T>(n))
-    return launch_radix_sort(k, n, desc, scratch, sb, device_info().sm_count, st);
+  if (use_radix<T>(n)) {
+    const int rc = launch_radix_sort(k, n, desc, scratch, sb, device_info().sm_count, st);
+    if (rc != B2P_ERR_UNSUPPORTED) return rc;  // (a device of more than 256 SMs: the merge sort)
+  }
   return desc ? launch_sort(k, n, Greater<T>{}, scratch, sb, st) : launch_sort(k, n, Less<T>{}, scratch, sb, st);
 }
 
