@@ -319,7 +319,9 @@ int b2p_sort(int dtype, void *keys, size_t n, int descending, void *scratch, siz
  * it).  The calls return after their work is complete (they synchronise
  * `stream`).  scratch: b2p_sharded_scratch_bytes(dtype, n, world) bytes,
  * zero-filled once (b2p_scratch_init), not shared with overlapping calls.
- * B2P_ERR_UNSUPPORTED when no libnccl.so.2 can be loaded. */
+ * B2P_ERR_UNSUPPORTED when no libnccl.so.2 can be loaded.  Every rank must
+ * make the call: a rank that rejects its arguments returns before the
+ * exchange, and the others then wait in NCCL until its timeout. */
 size_t b2p_sharded_scratch_bytes(int dtype, size_t n, int world);
 
 /* *out (device, accumulation type) = init op (the reduction of every rank's
