@@ -331,6 +331,12 @@ size_t b2p_sharded_scratch_bytes(int dtype, size_t n, int world);
 int b2p_sharded_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
                        void *scratch, size_t scratch_bytes, int config, void *nccl_comm, b2p_stream stream);
 
+/* *out = init + the dot product of the concatenated shards of a and b (each
+ * rank passes its shard of both; dtype F32, BF16 or F64; the compensated
+ * local dot of b2p_dot, partials combined in double). */
+int b2p_sharded_dot(int dtype, const void *a, const void *b, size_t n, void *out, const void *init,
+                    void *scratch, size_t scratch_bytes, int config, void *nccl_comm, b2p_stream stream);
+
 /* This rank's part of the inclusive (or exclusive) scan of the concatenated
  * shards: out[i] as the one-device scan of the whole array would give it.
  * The local scan runs once, with the combination of init and the totals of

@@ -89,6 +89,7 @@ def _declare(L):
         "b2p_sharded_scratch_bytes": ([i, sz, i], sz),
         "b2p_sharded_reduce": ([i, i, vp, sz, vp, vp, vp, sz, i, vp, vp], i),
         "b2p_sharded_scan": ([i, i, i, vp, vp, sz, vp, vp, sz, i, vp, vp], i),
+        "b2p_sharded_dot": ([i, vp, vp, sz, vp, vp, vp, sz, i, vp, vp], i),
         "b2p_shard_combine": ([i, i, vp, i, sz, vp, vp], i),
         "b2p_log_level": ([], i),
         "b2p_set_log_level": ([i], None),

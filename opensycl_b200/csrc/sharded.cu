@@ -1,4 +1,4 @@
-// Sharded reduce and scan over the ranks of an NCCL communicator, for C and
+// Sharded reduce, dot and scan over the ranks of an NCCL communicator, for C and
 // C++ hosts (one process or thread per GPU; rank r holds the r-th shard of
 // one logical array, rank order = element order).  The same single-exchange
 // plan as the Python layer (opensycl_b200/sharded.py):
@@ -17,6 +17,7 @@
 #include <dlfcn.h>
 #include <nccl.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -147,12 +148,14 @@ size_t local_part(size_t n, int dtype, int prim) {
   return (b + 255) / 256 * 256;
 }
 
-// The shard partial of every rank on the host: local reduce into this
-// rank's entry, one all-gather, one copy back.  entries: world * kEntry.
-int gather_partials(int dtype, int op, const void *in, size_t n, void *scratch, size_t scratch_bytes, int config,
-                    ncclComm_t comm, int world, cudaStream_t st, std::vector<unsigned char> &entries) {
+// The shard partial of every rank on the host: local reduce (or dot, when
+// `b` is given) into this rank's entry, one all-gather, one copy back.
+// entries: world * kEntry.
+int gather_partials(int dtype, int op, const void *in, const void *b, size_t n, void *scratch, size_t scratch_bytes,
+                    int config, ncclComm_t comm, int world, cudaStream_t st, std::vector<unsigned char> &entries) {
   const NcclApi &nc = nccl_api();
-  const size_t base = std::max(local_part(n, dtype, B2P_PRIM_REDUCE), local_part(n, dtype, B2P_PRIM_SCAN));
+  const size_t base = std::max({local_part(n, dtype, B2P_PRIM_REDUCE), local_part(n, dtype, B2P_PRIM_SCAN),
+                                local_part(n, dtype, B2P_PRIM_DOT)});
   if (scratch_bytes < base + 256 + kEntry * (size_t)world) return B2P_ERR_SCRATCH;
   unsigned char *mine = reinterpret_cast<unsigned char *>(scratch) + base;
   unsigned char *all = mine + 256;
@@ -160,7 +163,8 @@ int gather_partials(int dtype, int op, const void *in, size_t n, void *scratch, 
   cudaError_t e = cudaMemsetAsync(mine, 0, kEntry, st);
   if (e != cudaSuccess) return cuda_status(e);
   if (n > 0) {
-    const int rc = b2p_reduce(dtype, op, in, n, mine, nullptr, scratch, base, config, (b2p_stream)st);
+    const int rc = b ? b2p_dot(dtype, in, b, n, mine, nullptr, scratch, base, config, (b2p_stream)st)
+                     : b2p_reduce(dtype, op, in, n, mine, nullptr, scratch, base, config, (b2p_stream)st);
     if (rc) return rc;
   }
   if ((e = cudaMemcpyAsync(mine + 8, &flag, 8, cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_status(e);
@@ -197,8 +201,9 @@ extern "C" int b2p_shard_combine(int dtype, int op, const void *values, int coun
 
 extern "C" size_t b2p_sharded_scratch_bytes(int dtype, size_t n, int world) {
   if (world < 1) return 0;
-  return std::max(local_part(n, dtype, B2P_PRIM_REDUCE), local_part(n, dtype, B2P_PRIM_SCAN)) + 256 +
-         kEntry * (size_t)world + 256;
+  return std::max({local_part(n, dtype, B2P_PRIM_REDUCE), local_part(n, dtype, B2P_PRIM_SCAN),
+                   local_part(n, dtype, B2P_PRIM_DOT)}) +
+         256 + kEntry * (size_t)world + 256;
 }
 
 extern "C" int b2p_sharded_reduce(int dtype, int op, const void *in, size_t n, void *out, const void *init,
@@ -213,8 +218,8 @@ extern "C" int b2p_sharded_reduce(int dtype, int op, const void *in, size_t n, v
   if (!scratch) return cs.done(B2P_ERR_SCRATCH);
   cudaStream_t st = (cudaStream_t)stream;
   std::vector<unsigned char> entries;
-  if ((rc = gather_partials(dtype, op, in, n, scratch, scratch_bytes, config, (ncclComm_t)nccl_comm, world, st,
-                            entries)))
+  if ((rc = gather_partials(dtype, op, in, nullptr, n, scratch, scratch_bytes, config, (ncclComm_t)nccl_comm, world,
+                            st, entries)))
     return cs.done(rc);
   unsigned long long r = 0;
   rc = fold(dtype, op, entries.data(), entries.data() + 8, world, kEntry, init, &r);
@@ -239,8 +244,8 @@ extern "C" int b2p_sharded_scan(int dtype, int op, int inclusive, const void *in
   if (world == 1)  // nothing to exchange
     return cs.done(b2p_scan(dtype, op, inclusive, in, out, n, init, scratch, scratch_bytes, config, stream));
   std::vector<unsigned char> entries;
-  if ((rc = gather_partials(dtype, op, in, n, scratch, scratch_bytes, config, (ncclComm_t)nccl_comm, world, st,
-                            entries)))
+  if ((rc = gather_partials(dtype, op, in, nullptr, n, scratch, scratch_bytes, config, (ncclComm_t)nccl_comm, world,
+                            st, entries)))
     return cs.done(rc);
   if (n == 0) return cs.done(B2P_OK);
   // carry = init op totals of the ranks before this one
@@ -250,4 +255,27 @@ extern "C" int b2p_sharded_scan(int dtype, int op, int inclusive, const void *in
     return cs.done(b2p_scan(dtype, op, inclusive, in, out, n, nullptr, scratch, scratch_bytes, config, stream));
   if (rc) return cs.done(rc);
   return cs.done(b2p_scan(dtype, op, inclusive, in, out, n, &carry, scratch, scratch_bytes, config, stream));
+}
+
+extern "C" int b2p_sharded_dot(int dtype, const void *a, const void *b, size_t n, void *out, const void *init,
+                               void *scratch, size_t scratch_bytes, int config, void *nccl_comm, b2p_stream stream) {
+  CallScope cs("b2p_sharded_dot", dtype, n, 0, 2.0 * (double)n * dtype_size(dtype), stream);
+  if (dtype != B2P_F32 && dtype != B2P_BF16 && dtype != B2P_F64) return cs.done(B2P_ERR_UNSUPPORTED);
+  int world = 0, rank = 0;
+  int rc = comm_shape(nccl_comm, &world, &rank);
+  if (rc) return cs.done(rc);
+  if ((rc = check_pointer(out, acc_size(dtype)))) return cs.done(rc);
+  if (!scratch) return cs.done(B2P_ERR_SCRATCH);
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<unsigned char> entries;
+  if ((rc = gather_partials(dtype, B2P_SUM, a, b, n, scratch, scratch_bytes, config, (ncclComm_t)nccl_comm, world,
+                            st, entries)))
+    return cs.done(rc);
+  unsigned long long r = 0;
+  rc = fold(dtype, B2P_SUM, entries.data(), entries.data() + 8, world, kEntry, init, &r);
+  if (rc == B2P_ERR_INVALID_ARG) return cs.done(B2P_OK);  // every shard empty and no init: out untouched
+  if (rc) return cs.done(rc);
+  cudaError_t e = cudaMemcpyAsync(out, &r, acc_size(dtype), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return cs.done(cuda_status(e));
 }

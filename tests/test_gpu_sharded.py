@@ -112,6 +112,14 @@ def test_sharded_c_abi_single_rank(dev):
                 assert out.item() == ref.item()
             else:
                 assert abs(out.item() - ref.item()) <= 1e-6 * abs(ref.item()) + 1e-3
+            if code == C.F32:
+                x2 = torch.flip(x, [0]).contiguous()
+                od = torch.zeros(1, dtype=torch.float32, device="cuda")
+                assert L.b2p_sharded_dot(code, x.data_ptr(), x2.data_ptr(), n, od.data_ptr(), None,
+                                         scratch.data_ptr(), sb, C.AUTO, comm, sh) == C.OK
+                rd = C.dot(x, x2)
+                torch.cuda.synchronize()
+                assert abs(od.item() - rd.item()) <= 1e-6 * abs(rd.item()) + 1e-3
             y = torch.empty_like(x)
             assert L.b2p_sharded_scan(code, C.SUM, 1, x.data_ptr(), y.data_ptr(), n, None, scratch.data_ptr(), sb,
                                       C.AUTO, comm, sh) == C.OK
