@@ -39,6 +39,13 @@ namespace {
 // range holds their position.  A reduce needs no TMEM and no output
 // stages: only the per-thread words pass from reducers to emitters.
 
+// Double-float form of an FP64 value: hi its rounding to float, lo the
+// rounded rest.
+__device__ __forceinline__ DF df_of_f64(double d) {
+  const float h = (float)d;
+  return DF{h, (float)(d - (double)h)};
+}
+
 constexpr int kSegHasHead = 1;
 constexpr int kSegNeedCarry = 2;  // some output of the tile needs the carry
 // per-thread word from reducers to emitters
@@ -229,32 +236,104 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
       Acc r_end = P::identity();
       uint32_t w[kCols];
       constexpr int IPV = 16 / (int)sizeof(In), VPT = ITEMS / IPV, WPO = (int)sizeof(Out) / 4;
-      if (REDUCE && heads == 0 && ends == 0) {
-        // a reduce, no segment starts or ends here: only the thread total
-        // matters, folded in kChains independent chains (element j to chain
-        // j % kChains) so that the dependent additions overlap
-        constexpr int kChains = P::kCompensated ? 4 : 1;
-        Acc ch[kChains];
+      if constexpr (P::kCompensated) {
+        // fp32 / bf16 SUM: a thread's run is an FP64 sum of its values (32 at
+        // most, each exact in FP64), two instructions per element against
+        // the seven of a double-float TwoSum step; every output is one
+        // rounding of it, and the run goes on as (hi, lo), the FP64 value
+        // split into two floats
+        const double init_d = (double)init_acc.hi + (double)init_acc.lo;
+        double rd = 0.0;
+        if (REDUCE && heads == 0 && ends == 0) {
+          // a reduce, no segment starts or ends here: only the thread total
+          // matters, summed in four independent chains (element j to chain
+          // j % 4) so that the dependent additions overlap
+          double ch[4] = {0.0, 0.0, 0.0, 0.0};
+          if (lim == ITEMS) {
 #pragma unroll
-        for (int c = 0; c < kChains; ++c) ch[c] = P::identity();
+            for (int k = 0; k < VPT; ++k) {
+              const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+              const In *ev = reinterpret_cast<const In *>(&u);
+#pragma unroll
+              for (int q = 0; q < IPV; ++q) ch[(k * IPV + q) & 3] += (double)P::lift_f(ev[q]);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < VPT; ++k) {
+              const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+              const In *ev = reinterpret_cast<const In *>(&u);
+#pragma unroll
+              for (int q = 0; q < IPV; ++q)
+                if (k * IPV + q < lim) ch[(k * IPV + q) & 3] += (double)P::lift_f(ev[q]);
+            }
+          }
+          rd = (ch[0] + ch[1]) + (ch[2] + ch[3]);
+        } else if (!REDUCE && heads == 0) {
+          // a scan, no segment starts here (the common case inside long segments)
+#pragma unroll
+          for (int k = 0; k < VPT; ++k) {
+            const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+            const In *ev = reinterpret_cast<const In *>(&u);
+#pragma unroll
+            for (int q = 0; q < IPV; ++q) {
+              const int j = k * IPV + q;
+              const double x = j < lim ? (double)P::lift_f(ev[q]) : 0.0;
+              const Out o = (Out)(p.inclusive ? rd + x : rd);
+              rd += x;
+              memcpy(w + j * WPO, &o, sizeof(Out));
+            }
+          }
+        } else {
+          int ip = i0;                            // next boundary not yet passed (reduce)
+          long long seg = (long long)kb + i0 - 1;  // segment of the current run (reduce)
+#pragma unroll
+          for (int k = 0; k < VPT; ++k) {
+            const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
+            const In *ev = reinterpret_cast<const In *>(&u);
+#pragma unroll
+            for (int q = 0; q < IPV; ++q) {
+              const int j = k * IPV + q;
+              if ((heads >> j) & 1u) {
+                f = 1;
+                rd = init_d;
+                if constexpr (REDUCE) {
+                  // the segment starting here is the last boundary at e0 + j
+                  while (ip < m && B.at(ip) <= e0 + j) ++ip;
+                  seg = (long long)kb + ip - 1;
+                }
+              }
+              const double x = j < lim ? (double)P::lift_f(ev[q]) : 0.0;
+              if constexpr (REDUCE) {
+                rd += x;
+                if ((ends >> j) & 1u) {
+                  if (f) {
+                    out[seg] = (Out)rd;
+                  } else {
+                    j_end = j;
+                    r_end = df_of_f64(rd);
+                  }
+                }
+              } else {
+                const Out o = (Out)(p.inclusive ? rd + x : rd);
+                rd += x;
+                memcpy(w + j * WPO, &o, sizeof(Out));
+              }
+            }
+          }
+        }
+        run = df_of_f64(rd);
+      } else if (REDUCE && heads == 0 && ends == 0) {
+        // a reduce, no segment starts or ends here: only the thread total matters
         const bool full = lim == ITEMS;
 #pragma unroll
         for (int k = 0; k < VPT; ++k) {
           const uint4 u = *reinterpret_cast<const uint4 *>(buf + swz(t * VPT + k) * 16);
           const In *ev = reinterpret_cast<const In *>(&u);
 #pragma unroll
-          for (int q = 0; q < IPV; ++q) {
-            const int j = k * IPV + q;
-            if (full || j < lim) P::add(ch[j % kChains], ev[q]);
-          }
+          for (int q = 0; q < IPV; ++q)
+            if (full || k * IPV + q < lim) P::add(run, ev[q]);
         }
-        if constexpr (kChains == 4) {
-          ch[0] = P::combine(ch[0], ch[1]);
-          ch[2] = P::combine(ch[2], ch[3]);
-          ch[0] = P::combine(ch[0], ch[2]);
-        }
-        run = ch[0];
-      } else if (heads == 0 && !REDUCE) {
+      } else if (!REDUCE && heads == 0) {
         // a scan, no segment starts here (the common case inside long segments)
 #pragma unroll
         for (int k = 0; k < VPT; ++k) {
@@ -263,27 +342,15 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
 #pragma unroll
           for (int q = 0; q < IPV; ++q) {
             const int j = k * IPV + q;
-            const bool valid = j < lim;
-            Out o{};
-            if constexpr (P::kCompensated) {
-              const float x = valid ? P::lift_f(ev[q]) : 0.f;
-              if (p.inclusive) {
-                df_accumulate(run, x);
-                o = __fadd_rn(run.hi, run.lo);
-              } else {
-                o = __fadd_rn(run.hi, run.lo);
-                df_accumulate(run, x);
-              }
+            Out o;
+            if (p.inclusive) {
+              if (j < lim) P::add(run, ev[q]);
+              o = P::finalize(run);
             } else {
-              if (p.inclusive) {
-                if (valid) P::add(run, ev[q]);
-                o = P::finalize(run);
-              } else {
-                o = P::finalize(run);
-                if (valid) P::add(run, ev[q]);
-              }
+              o = P::finalize(run);
+              if (j < lim) P::add(run, ev[q]);
             }
-            if constexpr (!REDUCE) memcpy(w + j * WPO, &o, sizeof(Out));
+            memcpy(w + j * WPO, &o, sizeof(Out));
           }
         }
       } else {
@@ -306,24 +373,13 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
                 seg = (long long)kb + ip - 1;
               }
             }
-            Out o{};
-            if constexpr (P::kCompensated) {
-              const float x = valid ? P::lift_f(ev[q]) : 0.f;
-              if (p.inclusive) {
-                df_accumulate(run, x);
-                o = __fadd_rn(run.hi, run.lo);
-              } else {
-                o = __fadd_rn(run.hi, run.lo);
-                df_accumulate(run, x);
-              }
+            Out o;
+            if (p.inclusive) {
+              if (valid) P::add(run, ev[q]);
+              o = P::finalize(run);
             } else {
-              if (p.inclusive) {
-                if (valid) P::add(run, ev[q]);
-                o = P::finalize(run);
-              } else {
-                o = P::finalize(run);
-                if (valid) P::add(run, ev[q]);
-              }
+              o = P::finalize(run);
+              if (valid) P::add(run, ev[q]);
             }
             if constexpr (REDUCE) {
               if ((ends >> j) & 1u) {
@@ -340,7 +396,6 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
           }
         }
       }
-      if constexpr (P::kCompensated) run = df_norm(run);
       __syncwarp();
       if ((t & 31) == 0) mbar_arrive(&ps.empty[ri.s]);  // this warp is done with the input stage
       if constexpr (!REDUCE) {
@@ -399,7 +454,6 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
         // the tile's first segment and needs the tile's carry, which the
         // look-back warp adds
         if (j_end >= 0) {
-          if constexpr (P::kCompensated) r_end = df_norm(r_end);
           const Acc v = P::combine(tex.v, r_end);
           const long long sg = (long long)kb + i0 - 1;
           if (tex.f) {
