@@ -189,42 +189,52 @@ __global__ void __launch_bounds__(pipe_threads(NC), 1)
 // Reducer pass: the thread's ITEMS elements from the landed stage, their
 // running values from the identity (inclusive: after adding the element,
 // exclusive: before) as 32-bit words for TMEM, and the thread total.
+// Compensated sums (fp32 / bf16) run in FP64: the thread's values are exact
+// in FP64 and their sum far inside its precision, each parked word is one
+// rounding of the running value, and the total leaves as the double-float
+// (hi, lo) split of the FP64 sum.
 template <class P, int ITEMS, bool INCL>
 __device__ __forceinline__ typename P::Acc tmem_runs(const char *inbuf, uint32_t *w, int t) {
   using In = typename P::In;
   using Out = typename P::Out;
   constexpr int IPV = 16 / (int)sizeof(In), VPT = ITEMS / IPV, WPO = (int)sizeof(Out) / 4;
-  typename P::Acc run = P::identity();
+  if constexpr (P::kCompensated) {
+    double rd = 0.0;
 #pragma unroll
-  for (int k = 0; k < VPT; ++k) {
-    const uint4 u = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT + k) * 16);
-    const In *e = reinterpret_cast<const In *>(&u);
+    for (int k = 0; k < VPT; ++k) {
+      const uint4 u = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT + k) * 16);
+      const In *e = reinterpret_cast<const In *>(&u);
 #pragma unroll
-    for (int q = 0; q < IPV; ++q) {
-      Out o;
-      if constexpr (P::kCompensated) {
-        const float x = P::lift_f(e[q]);
-        if constexpr (INCL) {
-          df_accumulate(run, x);
-          o = __fadd_rn(run.hi, run.lo);
-        } else {
-          o = __fadd_rn(run.hi, run.lo);
-          df_accumulate(run, x);
-        }
-      } else {
-        if constexpr (INCL) {
-          P::add(run, e[q]);
-          o = P::finalize(run);
-        } else {
-          o = P::finalize(run);
-          P::add(run, e[q]);
-        }
+      for (int q = 0; q < IPV; ++q) {
+        const double x = (double)P::lift_f(e[q]);
+        const Out o = (Out)(INCL ? rd + x : rd);
+        rd += x;
+        memcpy(w + (k * IPV + q) * WPO, &o, sizeof(Out));
       }
-      memcpy(w + (k * IPV + q) * WPO, &o, sizeof(Out));
     }
+    const float h = (float)rd;
+    return typename P::Acc{h, (float)(rd - (double)h)};
+  } else {
+    typename P::Acc run = P::identity();
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+      const uint4 u = *reinterpret_cast<const uint4 *>(inbuf + swz(t * VPT + k) * 16);
+      const In *e = reinterpret_cast<const In *>(&u);
+#pragma unroll
+      for (int q = 0; q < IPV; ++q) {
+        Out o;
+        if constexpr (INCL) {
+          P::add(run, e[q]);
+          o = P::finalize(run);
+        } else {
+          o = P::finalize(run);
+          P::add(run, e[q]);
+        }
+        memcpy(w + (k * IPV + q) * WPO, &o, sizeof(Out));
+      }
+    }
+    return run;
   }
-  if constexpr (P::kCompensated) run = df_norm(run);
-  return run;
 }
 
 // Emitter pass: outputs = start combined with the parked running values,
