@@ -46,6 +46,14 @@ __device__ __forceinline__ DF df_of_f64(double d) {
   return DF{h, (float)(d - (double)h)};
 }
 
+// FP64 stand-in for a compensated policy in a tile's group scans (the
+// segmented operator over (flag, FP64 value) pairs)
+struct F64Sum {
+  using Acc = double;
+  __device__ static double identity() { return 0.0; }
+  __device__ static double combine(double a, double b) { return a + b; }
+};
+
 constexpr int kSegHasHead = 1;
 constexpr int kSegNeedCarry = 2;  // some output of the tile needs the carry
 // per-thread word from reducers to emitters
@@ -118,7 +126,8 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
   constexpr int kWorkWarps = REDUCE ? kGroups * NC / 32 : 2 * NC / 32;
   __shared__ Pair s_warp_g[kGroups][32];
   __shared__ Acc s_acc_g[kGroups][32];  // clean tiles: warp totals (reduce) or the scan's warp values
-  __shared__ double s_dbl_g[kGroups][32];  // clean tiles of a compensated reduce: FP64 warp totals
+  __shared__ double s_dbl_g[kGroups][32];  // clean tiles of a compensated sum: FP64 warp totals / values
+  __shared__ SegPair<F64Sum> s_pd_g[kGroups][32];  // compensated tiles with boundaries: FP64 warp values
   __shared__ int s_go[kGroups > 2 ? kGroups : 2];  // [g]: reducer group g; [1] of a scan: the emitters
   __shared__ int s_entering_end_g[kGroups];
   __shared__ long long s_stop[kGroups];  // reduce: the item at which each group met the end
@@ -426,7 +435,16 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
 #pragma unroll
           for (int w = 1; w < NC / 32; ++w) tile_tot = P::combine(tile_tot, s_acc[w]);
         } else {
-          const Acc tex = group_exclusive_scan_1bar<AccOps<P>, NC>(run, s_acc, &tile_tot, t, gbar);
+          Acc tex;
+          if constexpr (P::kCompensated) {
+            double tot_d;
+            const double ex_d =
+                group_exclusive_scan_1bar<F64Ops, NC>((double)run.hi + (double)run.lo, s_dbl_g[g], &tot_d, t, gbar);
+            tile_tot = df_of_f64(tot_d);
+            tex = df_of_f64(ex_d);
+          } else {
+            tex = group_exclusive_scan_1bar<AccOps<P>, NC>(run, s_acc, &tile_tot, t, gbar);
+          }
           texcl_all[(size_t)rs.s * NC + t] = tex;
           info_all[(size_t)rs.s * NC + t] = 0ull;
         }
@@ -446,8 +464,17 @@ __global__ void __launch_bounds__(seg_threads(NC, REDUCE), 1)
         if ((t & 31) == 0) mbar_arrive(&ps.slot_ready[rs.s]);
         continue;
       }
-      Pair tile_agg;
-      const Pair tex = group_exclusive_scan_1bar<SegOps<P>, NC>(Pair{run, f}, s_warp, &tile_agg, t, gbar);
+      Pair tile_agg, tex;
+      if constexpr (P::kCompensated) {
+        using PD = SegPair<F64Sum>;
+        PD agg_d;
+        const PD ex_d = group_exclusive_scan_1bar<SegOps<F64Sum>, NC>(PD{(double)run.hi + (double)run.lo, f},
+                                                                     s_pd_g[g], &agg_d, t, gbar);
+        tile_agg = Pair{df_of_f64(agg_d.v), agg_d.f};
+        tex = Pair{df_of_f64(ex_d.v), ex_d.f};
+      } else {
+        tex = group_exclusive_scan_1bar<SegOps<P>, NC>(Pair{run, f}, s_warp, &tile_agg, t, gbar);
+      }
       if constexpr (REDUCE) {
         // the segment entering this thread ends at j_end: after a head of an
         // earlier thread of the tile its value is complete; otherwise it is
